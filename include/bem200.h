@@ -1,0 +1,198 @@
+/*
+ * bem200 -- C ABI of the B200 retarded-BEM solver library (libbem200.so).
+ *
+ * Every entry point takes raw device pointers (e.g. torch.Tensor.data_ptr()),
+ * sizes and a CUDA stream (cudaStream_t passed as void*; NULL = default
+ * stream), enqueues its work on that stream and returns a status code
+ * (BEM200_OK = 0).  On failure the message is kept per host thread and read
+ * with bem200_last_error().  The caller owns all memory; functions that need
+ * scratch space take a workspace pointer whose size is given by the matching
+ * *_workspace_size query.  No entry point keeps global mutable state.
+ *
+ * Matrices are dense, row-major, complex (interleaved re/im), with leading
+ * dimension `ld` in elements.  Face arrays are (n, 3) row-major float64.
+ *
+ * The reference interface each group replaces (MNPBEM Python port v1.6.2):
+ *   refinement      -> mnpbem/greenfun/refine_utils.py:29 (refinematrix),
+ *                      mnpbem/greenfun/greenret_refined.py:122, :287
+ *                      (GreenRetRefined._refine_diagonal/_refine_offdiagonal),
+ *                      mnpbem/greenfun/compgreen_ret.py:192, :376 (closed surface)
+ *   assembly        -> mnpbem/greenfun/compgreen_ret.py:507 (CompGreenRet.eval)
+ *                      and mnpbem/greenfun/greenret_refined.py:654 (eval)
+ *   dense BEM       -> mnpbem/bem/bem_ret.py:293 (BEMRet.init), :1569 (solve)
+ *   operator        -> mnpbem/bem/bem_ret_iter.py:1362 (BEMRetIter._afun)
+ */
+#ifndef BEM200_H
+#define BEM200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BEM200_OK 0
+#define BEM200_ERR_ARG 1          /* invalid argument (size, pointer, option) */
+#define BEM200_ERR_CUDA 2         /* CUDA runtime error */
+#define BEM200_ERR_SINGULAR 3     /* exactly singular pivot met in an LU */
+#define BEM200_ERR_UNSUPPORTED 4  /* configuration not implemented */
+#define BEM200_ERR_TIMEOUT 5      /* a bounded device-side wait gave up */
+
+#define BEM200_C128 0 /* complex double, 16 bytes per element */
+#define BEM200_C64 1  /* complex float, 8 bytes per element */
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int bem200_version(void);
+
+/* Copies the calling thread's last error message into buf (always
+ * NUL-terminated when len > 0).  Returns the length of the message. */
+int bem200_last_error(char* buf, size_t len);
+
+/* ------------------------------------------------------------------ (a1)
+ * Refinement classification of all face pairs (i, j), i, j < n:
+ *   kind 2 if the centroids coincide (d == 0), kind 1 if
+ *   d - rad[j] < abs_cutoff or (d - rad[j]) / rad[i] < rel_cutoff, else 0,
+ * with d from |p_i|^2 + |p_j|^2 - 2 p_i.p_j (values below 1e-10 -> 0).
+ * Replaces refinematrix (mnpbem/greenfun/refine_utils.py:29-158).
+ * Pass 1 counts refined entries per row; bem200_scan_i32 turns counts into a
+ * CSR row pointer; pass 2 writes (row, col, kind) in row-major order. */
+int bem200_refine_count(int n, const double* pos, const double* rad, double abs_cutoff,
+                        double rel_cutoff, int32_t* row_count, void* stream);
+int bem200_scan_i32(int n, const int32_t* count, int64_t* row_ptr /* n + 1 */, void* stream);
+int bem200_refine_fill(int n, const double* pos, const double* rad, double abs_cutoff,
+                       double rel_cutoff, const int64_t* row_ptr, int32_t* ref_row,
+                       int32_t* ref_col, int8_t* ref_kind, void* stream);
+
+/* ------------------------------------------------------------- (a2, a3)
+ * Expansion coefficients of the refined entries, order+1 terms each:
+ *   g[e][m]     (nref, order+1)      Green function,  G = sum_m g_m (ik)^m
+ *   f[e][c][m]  (nref, 3, order+1)   Cartesian derivative, F = n_i . sum_m f_m (ik)^m
+ * kind 2 entries use the polar rule on face col (quadpol), kind 1 entries the
+ * 28-point rule on the (curved) sub-triangles of face col.
+ * nodes (n, 9, 3) and face_kind (n) describe every face:
+ *   0 flat triangle (nodes 0-2), 1 flat quad (0-3),
+ *   2 curved triangle [v0 v1 v2 e01 e12 e20], 3 curved quad [v0..v3 e01 e12 e23 e30 c].
+ * rules = [x28 y28 w28 | x3 y3 w3 | x4 y4 w4] with n28, n3, n4 points.
+ * Replaces GreenRetRefined._refine_diagonal / _refine_offdiagonal
+ * (mnpbem/greenfun/greenret_refined.py:122-516). */
+int bem200_refine_integrals(int64_t nref, const int32_t* ref_row, const int32_t* ref_col,
+                            const int8_t* ref_kind, const double* pos, const double* nvec,
+                            const double* tvec1, const double* tvec2, const double* area,
+                            const double* nodes, const int32_t* face_kind, const double* rules,
+                            int n28, int n3, int n4, int order, double* g, double* f,
+                            void* stream);
+
+/* ------------------------------------------------------------------ (a4)
+ * Closed-surface correction (Fuchs & Liu): for every face j of a particle
+ * whose closed surface is the set of particles closed_mask[pid[j]] (bit k =
+ * particle k; 0 = not closed)
+ *   c_j = -2 pi - sum_{i in surface} area_i F_ij / area_j ,
+ * F the quasistatic surface derivative (refined entries use n_i . f_0), and
+ * f[e][:, 0] += c_j n_j for the diagonal entry e = (j, j).  c is written to
+ * corr (n).  workspace: n doubles.
+ * Replaces CompGreenRet._initclosed / _apply_diag_corrections
+ * (mnpbem/greenfun/compgreen_ret.py:192-272, :376-400). */
+int bem200_closed_correction(int n, int npart, const int32_t* pid, const uint64_t* closed_mask,
+                             const double* pos, const double* nvec, const double* area,
+                             int64_t nref, const int64_t* row_ptr, const int32_t* ref_row,
+                             const int32_t* ref_col, const int8_t* ref_kind, int order,
+                             double* f, double* corr, void* stream);
+
+/* fn[e][m] = n_row(e) . f[e][:, m]  (the projection used by F / H1 / H2). */
+int bem200_refine_project(int64_t nref, const int32_t* ref_row, const double* nvec, int order,
+                          const double* f, double* fn, void* stream);
+
+/* ------------------------------------------------------------------ (a6)
+ * Per-wavelength assembly of the four BEM matrices
+ *   G1 = G[r00] - G[r10], G2 = G[r11] - G[r01], H1 = H1[r00] - H1[r10],
+ *   H2 = H2[r11] - H2[r01],
+ * where for particle block (a, b) region pair r connects with material
+ * blk_mat[(a * npart + b) * 4 + {0: r00, 1: r10, 2: r11, 3: r01}] (1-based,
+ * 0 = not connected) whose wavenumber is kmat_host[2 m], kmat_host[2 m + 1]
+ * (HOST array, nmat <= 16 materials).  G = area_j / d e^{ikd},
+ * F = (n_i . r)(ik - 1/d) / d^2 area_j e^{ikd}, H1/H2 = F +/- 2 pi on the
+ * diagonal of self blocks; refined entries take sum_m c_m (ik)^m e^{ikd}.
+ * out_dtype BEM200_C128 or BEM200_C64; any output pointer may be NULL.
+ * Replaces CompGreenRet.eval / _eval1 (mnpbem/greenfun/compgreen_ret.py:507,
+ * :739-858) and the G1/G2/H1/H2 build of BEMRet.init (bem_ret.py:407-423). */
+int bem200_green_assemble(int n, int npart, const int32_t* pid, const int32_t* blk_mat,
+                          int nmat, const double* kmat_host, const double* pos,
+                          const double* nvec, const double* area, int64_t nref,
+                          const int32_t* ref_row, const int32_t* ref_col, int order,
+                          const double* g, const double* fn, int out_dtype, void* G1, void* G2,
+                          void* H1, void* H2, int64_t ld, void* stream);
+
+/* ------------------------------------------------------------- dense LA
+ * Building blocks of the dense BEM (reference: the LU / lu_solve / matmul
+ * calls of mnpbem/bem/bem_ret.py:437-523, dispatched through
+ * mnpbem/utils/gpu.py:145-279).  dtype BEM200_C128 or BEM200_C64; engine 0 =
+ * CUDA cores, 1 = tcgen05 bf16x3 split (complex64 only), 2 = tcgen05 TF32
+ * (complex64 only).  alpha, beta: HOST pointers to (re, im).
+ * ws/ws_bytes: scratch for the tensor-core engines
+ * (bem200_gemm_workspace_size), may be NULL/0 for engine 0. */
+int bem200_gemm(int dtype, int engine, int m, int n, int k, const double* alpha, const void* A, int64_t lda,
+                const void* B, int64_t ldb, const double* beta, void* C, int64_t ldc, void* ws, size_t ws_bytes,
+                void* stream);
+size_t bem200_gemm_workspace_size(int engine, int m, int n, int k);
+/* In-place P A = L U with partial pivoting (largest |re|+|im|); ipiv[k] = row
+ * swapped with row k (0-based); *info = first zero pivot (1-based) or 0. */
+int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* ipiv, int32_t* info, void* ws,
+                 size_t ws_bytes, void* stream);
+/* B <- A^-1 B from the getrf factors (nrhs columns, row-major B). */
+int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t ld, const int32_t* ipiv, void* B,
+                 int64_t ldb, void* ws, size_t ws_bytes, void* stream);
+
+/* ------------------------------------------------------------- dense BEM
+ * precision 0 = complex128 throughout (the drop-in FP64 path);
+ * precision 1 = mixed: complex64 factors (GEMMs on `engine`) with FP64
+ * residuals and iterative refinement (bem200_bem_solve_ir).
+ * The workspace (bem200_bem_workspace_size bytes) holds the factors:
+ * LU(G1), LU(G2), Sigma1 = H1 G1^-1, LU(Delta), Delta^-1, LU(Sigma) + pivots.
+ * bem200_bem_slots returns where G1, G2, H1, H2 must be written (dtype of the
+ * precision) before bem200_bem_init, which consumes them.
+ * eps: eps_per_face = 0 -> eps1/eps2 are HOST (re, im) scalars of the inside /
+ * outside media; 1 -> device complex128 arrays (n) per face.
+ * Replaces BEMRet.init (mnpbem/bem/bem_ret.py:293-525). */
+size_t bem200_bem_workspace_size(int precision, int n);
+int bem200_bem_slots(int precision, int n, void* ws, void** G1, void** G2, void** H1, void** H2);
+int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face, const double* eps1,
+                    const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
+                    int32_t* info_host, void* stream);
+
+/* Right-hand side (complex128, row-major, npol polarisations):
+ *   b = [phi (n, p) | a (n, 3, p) | alpha (n, 3, p) | De (n, p)]  (8 n p values)
+ * solution W1 = [sig1 (n, p) | h1 (n, 3, p)] row-interleaved as n x 4p, W2 the
+ * same for (sig2, h2).  Replaces BEMRet.solve (mnpbem/bem/bem_ret.py:1569-1831,
+ * Eqs. 19-20 of Garcia de Abajo & Howie, PRB 65, 115418). */
+size_t bem200_bem_solve_workspace_size(int precision, int n, int npol);
+int bem200_bem_solve(int precision, int engine, int n, int npol, void* ws, const void* phi, const void* a,
+                     const void* alpha, const void* De, int eps_per_face, const double* eps1, const double* eps2,
+                     const double* nvec, double k0, void* W1, void* W2, void* scratch, void* gemm_ws,
+                     size_t gemm_ws_bytes, void* stream);
+
+/* Full FP64 BEM operator r = A x (b == NULL) or r = b - A x for x = (W1, W2):
+ * phi = G1 s1 - G2 s2, a = G1 h1 - G2 h2, alpha = H1 h1 - H2 h2 - ik n (G1 e1 s1
+ * - G2 e2 s2), De = H1 e1 s1 - H2 e2 s2 - ik n.(G1 e1 h1 - G2 e2 h2).
+ * Replaces BEMRetIter._afun (mnpbem/bem/bem_ret_iter.py:1362-1501). */
+size_t bem200_bem_apply_workspace_size(int n, int npol);
+int bem200_bem_apply(int n, int npol, const void* G1, const void* G2, const void* H1, const void* H2,
+                     int eps_per_face, const double* eps1, const double* eps2, const double* nvec, double k0,
+                     const void* W1, const void* W2, const void* b, void* r, void* scratch, void* stream);
+
+/* Mixed-precision solve: x = M b with the complex64 factors in ws, then
+ * x += M (b - A x) with the FP64 operator of G1..H2 (complex128) until
+ * max|b - A x| <= tol max|b| or maxit sweeps.  *iters, *relres: HOST outputs.
+ * This call synchronises the stream once per sweep to test convergence. */
+int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, const void* G2, const void* H1,
+                        const void* H2, const void* b, int eps_per_face, const double* eps1, const double* eps2,
+                        const double* nvec, double k0, double tol, int maxit, void* W1, void* W2, void* scratch,
+                        void* gemm_ws, size_t gemm_ws_bytes, int32_t* iters, double* relres, void* stream);
+
+/* dst (complex64) = src (complex128), count elements. */
+int bem200_convert_c128_c64(int64_t count, const void* src, void* dst, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BEM200_H */

@@ -1,0 +1,565 @@
+// Dense retarded BEM on one GPU: Sigma/Delta build, the solve of
+// Garcia de Abajo & Howie Eqs. (19, 20), the full FP64 BEM operator and the
+// mixed-precision (complex64 factors, FP64 residual) iterative refinement.
+//
+// Reference behaviour followed (MNPBEM Python port v1.6.2):
+//   BEMRet.init   mnpbem/bem/bem_ret.py:357-525 (MATLAB initmat.m:5-72)
+//   BEMRet.solve  mnpbem/bem/bem_ret.py:1569-1831 (MATLAB mldivide.m:29-49)
+//   _afun         mnpbem/bem/bem_ret_iter.py:1362-1501 (full operator)
+//
+// Workspace layout (element type C = complex128 for FP64, complex64 for the
+// mixed path), n x n matrices, ld = n:
+//   M0 G1 -> LU(G1)       M1 G2 -> LU(G2)      M2 H1 -> Sigma1
+//   M3 H2 -> Sigma2 -> (scratch)               M4 Delta -> LU(Delta)
+//   M5 Delta^-1           M6 Sigma -> LU(Sigma)
+//   pivots: 4 x n int32, then one device int (info)
+#include <vector>
+
+#include "dense.cuh"
+
+namespace bem200 {
+
+constexpr int kSlots = 7;
+
+template <typename C>
+struct BemState {
+  int n;
+  C* M[kSlots];
+  int32_t* piv[4];  // G1, G2, Delta, Sigma
+  int* info;
+};
+
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+template <typename C>
+static size_t state_bytes(int n) {
+  size_t mat = align256(sizeof(C) * (size_t)n * n);
+  return kSlots * mat + 4 * align256(sizeof(int32_t) * n) + 256;
+}
+
+template <typename C>
+static BemState<C> state_view(int n, void* ws) {
+  BemState<C> s;
+  s.n = n;
+  char* p = reinterpret_cast<char*>(ws);
+  size_t mat = align256(sizeof(C) * (size_t)n * n);
+  for (int i = 0; i < kSlots; ++i) s.M[i] = reinterpret_cast<C*>(p + i * mat);
+  p += kSlots * mat;
+  for (int i = 0; i < 4; ++i) {
+    s.piv[i] = reinterpret_cast<int32_t*>(p);
+    p += align256(sizeof(int32_t) * n);
+  }
+  s.info = reinterpret_cast<int*>(p);
+  return s;
+}
+
+// per-face or scalar eps (complex128 on the host side, converted per kernel)
+struct EpsArg {
+  int per_face;        // 0: scalar (e1, e2), 1: arrays d1, d2 (n complex128)
+  double2 e1, e2;
+  const double2* d1;
+  const double2* d2;
+};
+
+__device__ __forceinline__ double2 eps_at(const EpsArg& e, int i, bool second) {
+  if (!e.per_face) return second ? e.e2 : e.e1;
+  return second ? e.d2[i] : e.d1[i];
+}
+
+template <typename C>
+__device__ __forceinline__ C to_c(double2 v) {
+  return cmake<C>(v.x, v.y);
+}
+
+// ------------------------------------------------------------ init kernels
+template <typename C>
+__global__ void delta_kernel(long long nn, const C* __restrict__ S1, const C* __restrict__ S2, C* __restrict__ D) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nn) D[i] = csub(S1[i], S2[i]);
+}
+
+// Sigma_ij = Sigma1_ij e1_j - Sigma2_ij e2_j + k^2 L_i Dinv_ij (n_i . n_j) L_j,  L = e1 - e2
+template <typename C>
+__global__ void sigma_kernel(int n, const C* __restrict__ S1, const C* __restrict__ S2, const C* __restrict__ Dinv,
+                             const double* __restrict__ nvec, EpsArg eps, double k2, C* __restrict__ S) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * n) return;
+  int i = (int)(idx / n), j = (int)(idx % n);
+  double2 e1j = eps_at(eps, j, false), e2j = eps_at(eps, j, true);
+  double2 Li = csub(eps_at(eps, i, false), eps_at(eps, i, true));
+  double2 Lj = csub(e1j, e2j);
+  double nn = nvec[3 * i] * nvec[3 * j] + nvec[3 * i + 1] * nvec[3 * j + 1] + nvec[3 * i + 2] * nvec[3 * j + 2];
+  double2 s1 = make_double2(S1[idx].x, S1[idx].y), s2 = make_double2(S2[idx].x, S2[idx].y);
+  double2 di = make_double2(Dinv[idx].x, Dinv[idx].y);
+  double2 v = csub(cmul(s1, e1j), cmul(s2, e2j));
+  v = cadd(v, cscale(cmul(cmul(Li, di), Lj), k2 * nn));
+  S[idx] = to_c<C>(v);
+}
+
+template <typename C>
+static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, const double* nvec, double k0) {
+  BemState<C> s = state_view<C>(n, ws);
+  const long long nn = (long long)n * n;
+  LaContext c = ctx;
+  c.dinfo = s.info;
+  BEM_CUDA_CHECK(cudaMemsetAsync(s.info, 0, sizeof(int), ctx.stream));
+  int st;
+  // LU(G1), LU(G2)
+  if ((st = getrf<C>(c, n, s.M[0], n, s.piv[0]))) return st;
+  if ((st = getrf<C>(c, n, s.M[1], n, s.piv[1]))) return st;
+  // Sigma1 = H1 G1^-1, Sigma2 = H2 G2^-1 (right solves; M5 is scratch)
+  if ((st = solve_right<C>(c, n, n, s.M[0], n, s.piv[0], s.M[2], n, s.M[5]))) return st;
+  if ((st = solve_right<C>(c, n, n, s.M[1], n, s.piv[1], s.M[3], n, s.M[5]))) return st;
+  // Delta = Sigma1 - Sigma2, LU(Delta), Delta^-1
+  delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[4]);
+  BEM_LAUNCH_CHECK();
+  if ((st = getrf<C>(c, n, s.M[4], n, s.piv[2]))) return st;
+  if ((st = inverse<C>(c, n, s.M[4], n, s.piv[2], s.M[5], n))) return st;
+  // Sigma, LU(Sigma)
+  sigma_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(n, s.M[2], s.M[3], s.M[5], nvec, eps, k0 * k0, s.M[6]);
+  BEM_LAUNCH_CHECK();
+  if ((st = getrf<C>(c, n, s.M[6], n, s.piv[3]))) return st;
+  return BEM200_OK;
+}
+
+// ------------------------------------------------------------ solve kernels
+// RHS layout: phi (n, p), a (n, 3, p), alpha (n, 3, p), De (n, p), row-major.
+// Work arrays use W = [sigma-like (p) | h-like (3p)] rows of width 4p.
+
+// T = [L1 phi | a]  (n x 4p) for the Sigma1 product
+template <typename C>
+__global__ void solve_prep_kernel(int n, int p, const C* __restrict__ phi, const C* __restrict__ a, EpsArg eps,
+                                  C* __restrict__ T) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * 4 * p) return;
+  int i = (int)(idx / (4 * p)), c = (int)(idx % (4 * p));
+  if (c < p) {
+    double2 e1 = eps_at(eps, i, false);
+    C v = phi[(long long)i * p + c];
+    T[idx] = to_c<C>(cmul(e1, make_double2(v.x, v.y)));
+  } else {
+    T[idx] = a[(long long)i * 3 * p + (c - p)];
+  }
+}
+
+// alpha_m = alpha - (Sigma1 a) + ik n (L1 phi);  De_m = De - Sigma1 (L1 phi) + ik n.(L1 a)
+// S = Sigma1 T (n x 4p).  Output Am (n, 3p) and Dm (n, p).
+template <typename C>
+__global__ void solve_mod_kernel(int n, int p, const C* __restrict__ phi, const C* __restrict__ a,
+                                 const C* __restrict__ alpha, const C* __restrict__ De, const C* __restrict__ S,
+                                 const double* __restrict__ nvec, EpsArg eps, double k0, C* __restrict__ Am,
+                                 C* __restrict__ Dm) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * p) return;
+  int i = (int)(idx / p), q = (int)(idx % p);
+  double2 e1 = eps_at(eps, i, false);
+  const double2 ik = make_double2(0.0, k0);
+  double nv[3] = {nvec[3 * i], nvec[3 * i + 1], nvec[3 * i + 2]};
+  C ph = phi[(long long)i * p + q];
+  double2 L1phi = cmul(e1, make_double2(ph.x, ph.y));
+  const C* Si = S + (long long)i * 4 * p;
+  double2 dot = make_double2(0, 0);
+  for (int c = 0; c < 3; ++c) {
+    long long ai = ((long long)i * 3 + c) * p + q;
+    C al = alpha[ai];
+    C s = Si[p + c * p + q];
+    double2 v = csub(make_double2(al.x, al.y), make_double2(s.x, s.y));
+    v = cadd(v, cscale(cmul(ik, L1phi), nv[c]));
+    Am[ai] = to_c<C>(v);
+    C av = a[ai];
+    dot = cadd(dot, cscale(cmul(e1, make_double2(av.x, av.y)), nv[c]));
+  }
+  C de = De[idx];
+  C s0 = Si[q];
+  double2 v = csub(make_double2(de.x, de.y), make_double2(s0.x, s0.y));
+  v = cadd(v, cmul(ik, dot));
+  Dm[idx] = to_c<C>(v);
+}
+
+// rhs_sig = Dm + ik n.(L X),  X = Delta^-1 Am (n, 3p)
+template <typename C>
+__global__ void solve_rhs_sig_kernel(int n, int p, const C* __restrict__ Dm, const C* __restrict__ X,
+                                     const double* __restrict__ nvec, EpsArg eps, double k0, C* __restrict__ out) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * p) return;
+  int i = (int)(idx / p), q = (int)(idx % p);
+  double2 L = csub(eps_at(eps, i, false), eps_at(eps, i, true));
+  double2 dot = make_double2(0, 0);
+  for (int c = 0; c < 3; ++c) {
+    C x = X[((long long)i * 3 + c) * p + q];
+    dot = cadd(dot, cscale(make_double2(x.x, x.y), nvec[3 * i + c]));
+  }
+  C d = Dm[idx];
+  double2 v = cadd(make_double2(d.x, d.y), cmul(make_double2(0.0, k0), cmul(L, dot)));
+  out[idx] = to_c<C>(v);
+}
+
+// rhs_h = ik n (L sig2) + Am
+template <typename C>
+__global__ void solve_rhs_h_kernel(int n, int p, const C* __restrict__ sig2, const C* __restrict__ Am,
+                                   const double* __restrict__ nvec, EpsArg eps, double k0, C* __restrict__ out) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * 3 * p) return;
+  int i = (int)(idx / (3 * p)), c = (int)((idx / p) % 3), q = (int)(idx % p);
+  double2 L = csub(eps_at(eps, i, false), eps_at(eps, i, true));
+  C s = sig2[(long long)i * p + q];
+  C am = Am[idx];
+  double2 v = cadd(make_double2(am.x, am.y),
+                   cscale(cmul(make_double2(0.0, k0), cmul(L, make_double2(s.x, s.y))), nvec[3 * i + c]));
+  out[idx] = to_c<C>(v);
+}
+
+// W1 = [sig2 + phi | h2 + a],  W2 = [sig2 | h2]   (n x 4p)
+template <typename C>
+__global__ void solve_pack_kernel(int n, int p, const C* __restrict__ sig2, const C* __restrict__ h2,
+                                  const C* __restrict__ phi, const C* __restrict__ a, C* __restrict__ W1,
+                                  C* __restrict__ W2) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * 4 * p) return;
+  int i = (int)(idx / (4 * p)), c = (int)(idx % (4 * p));
+  C s, x;
+  if (c < p) {
+    s = sig2[(long long)i * p + c];
+    x = phi[(long long)i * p + c];
+  } else {
+    s = h2[(long long)i * 3 * p + (c - p)];
+    x = a[(long long)i * 3 * p + (c - p)];
+  }
+  W1[idx] = cadd(s, x);
+  W2[idx] = s;
+}
+
+template <typename C>
+static size_t solve_scratch_elems(int n, int p) {
+  return (size_t)n * p * 20;
+}
+
+// Solve for (W1 = [sig1 | h1], W2 = [sig2 | h2]) given RHS (phi, a, alpha, De)
+// in element type C.  scratch: solve_scratch_elems elements of C.
+template <typename C>
+static int bem_solve_core(const LaContext& ctx, int n, int p, void* ws, const C* phi, const C* a, const C* alpha,
+                          const C* De, const EpsArg& eps, const double* nvec, double k0, C* W1, C* W2, C* scratch) {
+  BemState<C> s = state_view<C>(n, ws);
+  cudaStream_t st_ = ctx.stream;
+  const long long np = (long long)n * p;
+  C* T = scratch;             // n x 4p
+  C* S = T + 4 * np;          // n x 4p
+  C* Am = S + 4 * np;         // n x 3p
+  C* Dm = Am + 3 * np;        // n x p
+  C* X = Dm + np;             // n x 3p
+  C* rs = X + 3 * np;         // n x p
+  C* h2 = rs + np;            // n x 3p   (total 20 np)
+  const C one = cmake<C>(1.0, 0.0), zero = czero<C>();
+  int st;
+  solve_prep_kernel<C><<<ceil_div(4 * np, 256), 256, 0, st_>>>(n, p, phi, a, eps, T);
+  BEM_LAUNCH_CHECK();
+  if ((st = gemm<C>(ctx, n, 4 * p, n, one, s.M[2], n, T, 4 * p, zero, S, 4 * p))) return st;
+  solve_mod_kernel<C><<<ceil_div(np, 256), 256, 0, st_>>>(n, p, phi, a, alpha, De, S, nvec, eps, k0, Am, Dm);
+  BEM_LAUNCH_CHECK();
+  // X = Delta^-1 Am
+  if ((st = gemm<C>(ctx, n, 3 * p, n, one, s.M[5], n, Am, 3 * p, zero, X, 3 * p))) return st;
+  solve_rhs_sig_kernel<C><<<ceil_div(np, 256), 256, 0, st_>>>(n, p, Dm, X, nvec, eps, k0, rs);
+  BEM_LAUNCH_CHECK();
+  // sig2 = Sigma^-1 rs   (in place in rs)
+  if ((st = solve_left<C>(ctx, n, p, s.M[6], n, s.piv[3], rs, p))) return st;
+  // h2 = Delta^-1 (ik n L sig2 + Am)
+  solve_rhs_h_kernel<C><<<ceil_div(3 * np, 256), 256, 0, st_>>>(n, p, rs, Am, nvec, eps, k0, X);
+  BEM_LAUNCH_CHECK();
+  if ((st = gemm<C>(ctx, n, 3 * p, n, one, s.M[5], n, X, 3 * p, zero, h2, 3 * p))) return st;
+  solve_pack_kernel<C><<<ceil_div(4 * np, 256), 256, 0, st_>>>(n, p, rs, h2, phi, a, W1, W2);
+  BEM_LAUNCH_CHECK();
+  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[0], n, s.piv[0], W1, 4 * p))) return st;
+  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[1], n, s.piv[1], W2, 4 * p))) return st;
+  return BEM200_OK;
+}
+
+// ------------------------------------------------------------ FP64 operator
+// U = [s | h | e s | e h] (n x 8p) from W = [s | h] (n x 4p)
+__global__ void op_prep_kernel(int n, int p, const double2* __restrict__ W, EpsArg eps, bool second,
+                               double2* __restrict__ U) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * 8 * p) return;
+  int i = (int)(idx / (8 * p)), c = (int)(idx % (8 * p));
+  double2 w = W[(long long)i * 4 * p + (c % (4 * p))];
+  U[idx] = (c < 4 * p) ? w : cmul(eps_at(eps, i, second), w);
+}
+
+// r = b - A x with GU1 = G1 U1, GU2 = G2 U2, HU1 = H1 U1, HU2 = H2 U2 (n x 8p):
+//   phi   = G1 s1 - G2 s2                          a  = G1 h1 - G2 h2
+//   alpha = H1 h1 - H2 h2 - ik n (G1 e1 s1 - G2 e2 s2)
+//   De    = H1 e1 s1 - H2 e2 s2 - ik n.(G1 e1 h1 - G2 e2 h2)
+// b and r use the RHS layout (phi, a, alpha, De); when b is null, r = A x.
+__global__ void op_combine_kernel(int n, int p, const double2* __restrict__ GU1, const double2* __restrict__ GU2,
+                                  const double2* __restrict__ HU1, const double2* __restrict__ HU2,
+                                  const double* __restrict__ nvec, double k0, const double2* __restrict__ bphi,
+                                  const double2* __restrict__ ba, const double2* __restrict__ balpha,
+                                  const double2* __restrict__ bDe, double2* __restrict__ rphi,
+                                  double2* __restrict__ ra, double2* __restrict__ ralpha, double2* __restrict__ rDe) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * p) return;
+  int i = (int)(idx / p), q = (int)(idx % p);
+  const int w8 = 8 * p;
+  const double2* g1 = GU1 + (long long)i * w8;
+  const double2* g2 = GU2 + (long long)i * w8;
+  const double2* h1 = HU1 + (long long)i * w8;
+  const double2* h2 = HU2 + (long long)i * w8;
+  const double2 ik = make_double2(0.0, k0);
+  const double nv[3] = {nvec[3 * i], nvec[3 * i + 1], nvec[3 * i + 2]};
+  const double sgn = bphi ? -1.0 : 1.0;
+  // columns: s -> q, h_c -> p + c p + q, e s -> 4p + q, e h_c -> 5p + c p + q
+  double2 phi = csub(g1[q], g2[q]);
+  double2 Ges = csub(g1[4 * p + q], g2[4 * p + q]);
+  double2 De = csub(h1[4 * p + q], h2[4 * p + q]);
+  double2 dotGeh = make_double2(0, 0);
+  for (int c = 0; c < 3; ++c) {
+    int hc = p + c * p + q;
+    double2 av = csub(g1[hc], g2[hc]);
+    double2 al = csub(csub(h1[hc], h2[hc]), cscale(cmul(ik, Ges), nv[c]));
+    dotGeh = cadd(dotGeh, cscale(csub(g1[4 * p + hc], g2[4 * p + hc]), nv[c]));
+    long long ai = ((long long)i * 3 + c) * p + q;
+    ra[ai] = bphi ? csub(ba[ai], av) : av;
+    ralpha[ai] = bphi ? csub(balpha[ai], al) : al;
+  }
+  De = csub(De, cmul(ik, dotGeh));
+  rphi[idx] = bphi ? csub(bphi[idx], phi) : phi;
+  rDe[idx] = bphi ? csub(bDe[idx], De) : De;
+  (void)sgn;
+}
+
+// A x (or b - A x) for x = (W1 = [s1|h1], W2 = [s2|h2]); scratch: 40 n p complex128
+static int bem_apply(const LaContext& ctx, int n, int p, const double2* G1, const double2* G2, const double2* H1,
+                     const double2* H2, const EpsArg& eps, const double* nvec, double k0, const double2* W1,
+                     const double2* W2, const double2* b /* 8np or null */, double2* r /* 8np */,
+                     double2* scratch) {
+  const long long np = (long long)n * p;
+  double2* U1 = scratch;
+  double2* U2 = U1 + 8 * np;
+  double2* GU1 = U2 + 8 * np;
+  double2* GU2 = GU1 + 8 * np;
+  double2* HU1 = GU2 + 8 * np;
+  op_prep_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(n, p, W1, eps, false, U1);
+  BEM_LAUNCH_CHECK();
+  op_prep_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(n, p, W2, eps, true, U2);
+  BEM_LAUNCH_CHECK();
+  const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
+  int st;
+  if ((st = gemm<double2>(ctx, n, 8 * p, n, one, G1, n, U1, 8 * p, zero, GU1, 8 * p))) return st;
+  if ((st = gemm<double2>(ctx, n, 8 * p, n, one, G2, n, U2, 8 * p, zero, GU2, 8 * p))) return st;
+  if ((st = gemm<double2>(ctx, n, 8 * p, n, one, H1, n, U1, 8 * p, zero, HU1, 8 * p))) return st;
+  // U1 is free now: reuse it for H2 U2
+  if ((st = gemm<double2>(ctx, n, 8 * p, n, one, H2, n, U2, 8 * p, zero, U1, 8 * p))) return st;
+  const double2* bp = b;
+  op_combine_kernel<<<ceil_div(np, 256), 256, 0, ctx.stream>>>(
+      n, p, GU1, GU2, HU1, U1, nvec, k0, bp, bp ? bp + np : nullptr, bp ? bp + 4 * np : nullptr,
+      bp ? bp + 7 * np : nullptr, r, r + np, r + 4 * np, r + 7 * np);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+// ------------------------------------------------------------ mixed IR
+__global__ void c128_to_c64_kernel(long long n, const double2* __restrict__ x, float2* __restrict__ y, double scale) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = make_float2((float)(x[i].x * scale), (float)(x[i].y * scale));
+}
+__global__ void axpy_c64_to_c128_kernel(long long n, const float2* __restrict__ x, double scale,
+                                        double2* __restrict__ y, bool accumulate) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double2 v = make_double2((double)x[i].x * scale, (double)x[i].y * scale);
+  y[i] = accumulate ? cadd(y[i], v) : v;
+}
+// max |re|, |im| over a vector (non-negative doubles compare as integers)
+__global__ void absmax_kernel(long long n, const double2* __restrict__ x, unsigned long long* __restrict__ out) {
+  double m = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, fmax(fabs(x[i].x), fabs(x[i].y)));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+static int absmax_host(cudaStream_t s, long long n, const double2* x, unsigned long long* dscratch, double* out) {
+  BEM_CUDA_CHECK(cudaMemsetAsync(dscratch, 0, sizeof(unsigned long long), s));
+  absmax_kernel<<<296, 256, 0, s>>>(n, x, dscratch);
+  BEM_LAUNCH_CHECK();
+  unsigned long long h = 0;
+  BEM_CUDA_CHECK(cudaMemcpyAsync(&h, dscratch, sizeof(h), cudaMemcpyDeviceToHost, s));
+  BEM_CUDA_CHECK(cudaStreamSynchronize(s));
+  double d;
+  memcpy(&d, &h, sizeof(d));
+  *out = d;
+  return BEM200_OK;
+}
+
+}  // namespace bem200
+
+using namespace bem200;
+
+static EpsArg make_eps(int per_face, const double* e1, const double* e2) {
+  EpsArg e;
+  e.per_face = per_face;
+  e.d1 = nullptr;
+  e.d2 = nullptr;
+  if (per_face) {
+    e.d1 = reinterpret_cast<const double2*>(e1);
+    e.d2 = reinterpret_cast<const double2*>(e2);
+    e.e1 = e.e2 = make_double2(0, 0);
+  } else {
+    e.e1 = make_double2(e1[0], e1[1]);
+    e.e2 = make_double2(e2[0], e2[1]);
+  }
+  return e;
+}
+
+static GemmEngine engine_from(int e) {
+  return e == 1 ? GemmEngine::kTcBf16x3 : (e == 2 ? GemmEngine::kTcTf32 : GemmEngine::kSimt);
+}
+
+extern "C" {
+
+size_t bem200_bem_workspace_size(int precision, int n) {
+  return precision == 0 ? state_bytes<double2>(n) : state_bytes<float2>(n);
+}
+
+int bem200_bem_slots(int precision, int n, void* ws, void** G1, void** G2, void** H1, void** H2) {
+  BEM_REQUIRE(ws && n > 0, BEM200_ERR_ARG, "bem_slots: bad arguments");
+  if (precision == 0) {
+    BemState<double2> s = state_view<double2>(n, ws);
+    *G1 = s.M[0]; *G2 = s.M[1]; *H1 = s.M[2]; *H2 = s.M[3];
+  } else {
+    BemState<float2> s = state_view<float2>(n, ws);
+    *G1 = s.M[0]; *G2 = s.M[1]; *H1 = s.M[2]; *H2 = s.M[3];
+  }
+  return BEM200_OK;
+}
+
+int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face, const double* eps1,
+                    const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
+                    int32_t* info_host, void* stream) {
+  BEM_REQUIRE(n > 0 && ws && eps1 && eps2 && nvec, BEM200_ERR_ARG, "bem_init: bad arguments");
+  LaContext ctx;
+  ctx.stream = (cudaStream_t)stream;
+  ctx.engine = engine_from(engine);
+  ctx.ws = gemm_ws;
+  ctx.ws_bytes = gemm_ws_bytes;
+  EpsArg eps = make_eps(eps_per_face, eps1, eps2);
+  int st = precision == 0 ? bem_init_t<double2>(ctx, n, ws, eps, nvec, k0) : bem_init_t<float2>(ctx, n, ws, eps, nvec, k0);
+  if (st) return st;
+  if (info_host) {
+    int* dinfo = precision == 0 ? state_view<double2>(n, ws).info : state_view<float2>(n, ws).info;
+    BEM_CUDA_CHECK(cudaMemcpyAsync(info_host, dinfo, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    BEM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
+    BEM_REQUIRE(*info_host == 0, BEM200_ERR_SINGULAR, "bem_init: exactly singular pivot at column %d", *info_host);
+  }
+  return BEM200_OK;
+}
+
+size_t bem200_bem_solve_workspace_size(int precision, int n, int npol) {
+  size_t np = (size_t)n * npol;
+  if (precision == 0) return sizeof(double2) * 20 * np;
+  // mixed: c64 core scratch + c64 rhs/solution + c128 IR vectors + operator scratch
+  return sizeof(float2) * (20 * np + 16 * np) + sizeof(double2) * (8 * np * 3 + 40 * np) + 256;
+}
+
+int bem200_bem_solve(int precision, int engine, int n, int npol, void* ws, const void* phi, const void* a,
+                     const void* alpha, const void* De, int eps_per_face, const double* eps1, const double* eps2,
+                     const double* nvec, double k0, void* W1, void* W2, void* scratch, void* gemm_ws,
+                     size_t gemm_ws_bytes, void* stream) {
+  BEM_REQUIRE(precision == 0, BEM200_ERR_ARG, "bem_solve: use bem200_bem_solve_ir for the mixed path");
+  BEM_REQUIRE(n > 0 && npol > 0 && ws && phi && a && alpha && De && W1 && W2 && scratch, BEM200_ERR_ARG,
+              "bem_solve: bad arguments");
+  LaContext ctx;
+  ctx.stream = (cudaStream_t)stream;
+  ctx.engine = engine_from(engine);
+  ctx.ws = gemm_ws;
+  ctx.ws_bytes = gemm_ws_bytes;
+  EpsArg eps = make_eps(eps_per_face, eps1, eps2);
+  return bem_solve_core<double2>(ctx, n, npol, ws, (const double2*)phi, (const double2*)a, (const double2*)alpha,
+                                 (const double2*)De, eps, nvec, k0, (double2*)W1, (double2*)W2, (double2*)scratch);
+}
+
+int bem200_bem_apply(int n, int npol, const void* G1, const void* G2, const void* H1, const void* H2,
+                     int eps_per_face, const double* eps1, const double* eps2, const double* nvec, double k0,
+                     const void* W1, const void* W2, const void* b, void* r, void* scratch, void* stream) {
+  BEM_REQUIRE(n > 0 && npol > 0 && G1 && G2 && H1 && H2 && W1 && W2 && r && scratch, BEM200_ERR_ARG,
+              "bem_apply: bad arguments");
+  LaContext ctx;
+  ctx.stream = (cudaStream_t)stream;
+  EpsArg eps = make_eps(eps_per_face, eps1, eps2);
+  return bem_apply(ctx, n, npol, (const double2*)G1, (const double2*)G2, (const double2*)H1, (const double2*)H2, eps,
+                   nvec, k0, (const double2*)W1, (const double2*)W2, (const double2*)b, (double2*)r,
+                   (double2*)scratch);
+}
+
+int bem200_convert_c128_c64(int64_t count, const void* src, void* dst, void* stream) {
+  BEM_REQUIRE(count >= 0 && (count == 0 || (src && dst)), BEM200_ERR_ARG, "convert: bad arguments");
+  if (count == 0) return BEM200_OK;
+  c128_to_c64_kernel<<<ceil_div(count, 256), 256, 0, (cudaStream_t)stream>>>(count, (const double2*)src,
+                                                                             (float2*)dst, 1.0);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+size_t bem200_bem_apply_workspace_size(int n, int npol) { return sizeof(double2) * 40 * (size_t)n * npol; }
+
+int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, const void* G2, const void* H1,
+                        const void* H2, const void* b, int eps_per_face, const double* eps1, const double* eps2,
+                        const double* nvec, double k0, double tol, int maxit, void* W1, void* W2, void* scratch,
+                        void* gemm_ws, size_t gemm_ws_bytes, int32_t* iters, double* relres, void* stream) {
+  BEM_REQUIRE(n > 0 && npol > 0 && ws && G1 && G2 && H1 && H2 && b && W1 && W2 && scratch && iters && relres,
+              BEM200_ERR_ARG, "bem_solve_ir: bad arguments");
+  LaContext ctx;
+  ctx.stream = (cudaStream_t)stream;
+  ctx.engine = engine_from(engine);
+  ctx.ws = gemm_ws;
+  ctx.ws_bytes = gemm_ws_bytes;
+  EpsArg eps = make_eps(eps_per_face, eps1, eps2);
+  const long long np = (long long)n * npol;
+  char* p = reinterpret_cast<char*>(scratch);
+  float2* core = reinterpret_cast<float2*>(p);        p += sizeof(float2) * 20 * np;
+  float2* rhs32 = reinterpret_cast<float2*>(p);       p += sizeof(float2) * 8 * np;
+  float2* sol32 = reinterpret_cast<float2*>(p);       p += sizeof(float2) * 8 * np;
+  double2* r = reinterpret_cast<double2*>(p);         p += sizeof(double2) * 8 * np;
+  double2* x = reinterpret_cast<double2*>(p);         p += sizeof(double2) * 8 * np;
+  p += sizeof(double2) * 8 * np;  // reserved
+  double2* opws = reinterpret_cast<double2*>(p);      p += sizeof(double2) * 40 * np;
+  unsigned long long* red = reinterpret_cast<unsigned long long*>(p);
+  cudaStream_t s = ctx.stream;
+  const double2* bb = (const double2*)b;
+  double bnorm = 0;
+  int st = absmax_host(s, 8 * np, bb, red, &bnorm);
+  if (st) return st;
+  BEM_REQUIRE(bnorm > 0 && bnorm < 1e300, BEM200_ERR_ARG, "bem_solve_ir: right-hand side is zero or not finite");
+  // x = M b  (mixed solve, scaled to unit magnitude)
+  const double2* res = bb;
+  double rnorm = bnorm;
+  int it = 0;
+  bool first = true;
+  while (true) {
+    double scale = 1.0 / rnorm;
+    c128_to_c64_kernel<<<ceil_div(8 * np, 256), 256, 0, s>>>(8 * np, res, rhs32, scale);
+    BEM_LAUNCH_CHECK();
+    // rhs32 = [phi (np) | a (3np) | alpha (3np) | De (np)];  sol32 = [W1 (4np) | W2 (4np)]
+    if ((st = bem_solve_core<float2>(ctx, n, npol, ws, rhs32, rhs32 + np, rhs32 + 4 * np, rhs32 + 7 * np, eps, nvec,
+                                     k0, sol32, sol32 + 4 * np, core)))
+      return st;
+    axpy_c64_to_c128_kernel<<<ceil_div(8 * np, 256), 256, 0, s>>>(8 * np, sol32, rnorm, x, !first);
+    BEM_LAUNCH_CHECK();
+    first = false;
+    // r = b - A x
+    if ((st = bem_apply(ctx, n, npol, (const double2*)G1, (const double2*)G2, (const double2*)H1, (const double2*)H2,
+                        eps, nvec, k0, x, x + 4 * np, bb, r, opws)))
+      return st;
+    if ((st = absmax_host(s, 8 * np, r, red, &rnorm))) return st;
+    ++it;
+    if (!(rnorm <= tol * bnorm) && !(rnorm < 1e300)) break;  // NaN / overflow: stop
+    if (rnorm <= tol * bnorm || it >= maxit) break;
+    res = r;
+  }
+  *iters = it;
+  *relres = rnorm / bnorm;
+  BEM_CUDA_CHECK(cudaMemcpyAsync(W1, x, sizeof(double2) * 4 * np, cudaMemcpyDeviceToDevice, s));
+  BEM_CUDA_CHECK(cudaMemcpyAsync(W2, x + 4 * np, sizeof(double2) * 4 * np, cudaMemcpyDeviceToDevice, s));
+  return BEM200_OK;
+}
+
+}  // extern "C"

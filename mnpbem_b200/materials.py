@@ -1,0 +1,98 @@
+"""Dielectric functions eps(lambda) and wavenumbers k = 2 pi / lambda * sqrt(eps).
+
+Calling convention of the reference materials: ``eps, k = material(enei)``
+with ``enei`` the vacuum wavelength in nm (reference
+mnpbem/materials/eps_const.py:48-72, eps_drude.py:73-107, eps_table.py:114-152).
+"""
+import os
+
+import numpy as np
+
+#: eV <-> nm conversion used by the reference (mnpbem/utils/constants.py:9)
+EV2NM = 1.0 / 8.0655477e-4
+
+
+class EpsConst:
+    """Wavelength-independent dielectric constant."""
+
+    def __init__(self, eps):
+        if eps is None or not np.isscalar(eps):
+            raise TypeError("EpsConst: 'eps' must be a numeric value")
+        self.eps = eps
+
+    def __call__(self, enei):
+        enei = np.asarray(enei)
+        eps = np.full_like(enei, self.eps, dtype=complex)
+        return eps, 2 * np.pi / enei * np.sqrt(eps)
+
+    def __repr__(self):
+        return "EpsConst({})".format(self.eps)
+
+
+class EpsDrude:
+    """Drude metal eps = eps0 - wp^2 / (w (w + i gammad)), energies in eV."""
+
+    def __init__(self, eps0, wp, gammad, name=None):
+        self.eps0, self.wp, self.gammad, self.name = eps0, wp, gammad, name
+
+    def __call__(self, enei):
+        enei = np.asarray(enei, dtype=float)
+        w = EV2NM / enei
+        eps = self.eps0 - self.wp ** 2 / (w * (w + 1j * self.gammad))
+        return eps, 2 * np.pi / enei * np.sqrt(eps)
+
+    def __repr__(self):
+        return "EpsDrude({}, {}, {})".format(self.eps0, self.wp, self.gammad)
+
+
+class EpsTable:
+    """Tabulated refractive index (columns: energy [eV], n, k), cubic-spline
+    interpolated in wavelength; eps = (n + i k)^2.  Raises ValueError outside
+    the tabulated range, like the reference."""
+
+    def __init__(self, filename):
+        from scipy.interpolate import CubicSpline
+        if not os.path.exists(filename):
+            raise FileNotFoundError("Material data file not found: {}".format(filename))
+        rows = []
+        with open(filename) as f:
+            for line in f:
+                line = line.strip()
+                if not line or line[0] in "%#":
+                    continue
+                try:
+                    vals = [float(x) for x in line.split()]
+                except ValueError:
+                    continue
+                if len(vals) >= 3:
+                    rows.append(vals[:3])
+        data = np.array(rows)
+        enei = EV2NM / data[:, 0]
+        order = np.argsort(enei)
+        self.enei = enei[order]
+        self.ni = CubicSpline(self.enei, data[order, 1])
+        self.ki = CubicSpline(self.enei, data[order, 2])
+
+    def __call__(self, enei):
+        enei = np.asarray(enei, dtype=float)
+        if np.any(enei < self.enei.min()) or np.any(enei > self.enei.max()):
+            raise ValueError("Wavelength out of range. Valid range: {:.1f} - {:.1f} nm".format(
+                self.enei.min(), self.enei.max()))
+        eps = (self.ni(enei) + 1j * self.ki(enei)) ** 2
+        return eps, 2 * np.pi / enei * np.sqrt(eps)
+
+
+class EpsValues:
+    """Dielectric function given by a lookup {wavelength: eps}; used to drive a
+    solve with eps values computed elsewhere (e.g. sampled from a table)."""
+
+    def __init__(self, table):
+        self.table = {float(k): complex(v) for k, v in dict(table).items()}
+
+    def __call__(self, enei):
+        e = float(np.asarray(enei).ravel()[0])
+        for key, val in self.table.items():
+            if abs(key - e) <= 1e-9 * max(1.0, abs(e)):
+                eps = np.asarray(val, dtype=complex)
+                return eps, 2 * np.pi / np.asarray(enei, dtype=float) * np.sqrt(eps)
+        raise ValueError("EpsValues: no value tabulated at {} nm".format(e))

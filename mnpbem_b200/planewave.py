@@ -1,0 +1,150 @@
+"""Plane-wave excitation, far fields and cross sections (host side).
+
+Mirrors ``PlaneWaveRet`` (mnpbem/simulation/planewave_ret.py:17) and
+``SpectrumRet`` (mnpbem/spectrum/spectrum_ret.py:136): ``potential(p, enei)``
+gives the vector potentials on both sides of every face, ``extinction``
+uses the optical theorem and ``scattering`` integrates the Poynting vector
+over the 256-direction unit sphere.  These are O(N) per polarisation and run
+on the host, as in the reference.
+"""
+import os
+
+import numpy as np
+
+_DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+
+
+class CompStruct:
+    """Attribute container with dict-style access (reference compgreen_stat.py:1154)."""
+
+    def __init__(self, p, enei, **fields):
+        self.p = p
+        self.enei = enei
+        for k, v in fields.items():
+            setattr(self, k, v)
+
+    def set(self, **fields):
+        for k, v in fields.items():
+            setattr(self, k, v)
+        return self
+
+    def get(self, name, default=None):
+        return getattr(self, name, default)
+
+    def __getitem__(self, name):
+        return getattr(self, name)
+
+    def __contains__(self, name):
+        return hasattr(self, name)
+
+
+def _pinfty():
+    d = np.load(os.path.join(_DATA, "pinfty256.npz"))
+    return d["nvec"], d["area"]
+
+
+class SpectrumRet:
+    """Far fields on a discretised unit sphere (default: the 256-direction sphere)."""
+
+    def __init__(self, pinfty=None, medium=1):
+        self.medium = medium
+        if pinfty is None:
+            self.nvec, self.area = _pinfty()
+        else:
+            self.nvec = np.atleast_2d(np.asarray(pinfty.nvec if hasattr(pinfty, "nvec") else pinfty, dtype=float))
+            self.area = (np.asarray(pinfty.area) if hasattr(pinfty, "area")
+                         else np.full(len(self.nvec), 4 * np.pi / len(self.nvec)))
+        self.ndir = len(self.nvec)
+
+    def farfield(self, sig, direction=None):
+        """e, h (ndir, 3, p) far-field amplitudes (spectrum_ret.py:231-392)."""
+        dirs = self.nvec if direction is None else np.atleast_2d(np.asarray(direction, dtype=float))
+        p = sig.p
+        enei = sig.enei
+        k = complex(np.asarray(p.eps[self.medium - 1](enei)[1]).ravel()[0])
+        k0 = 2 * np.pi / enei
+        phase = np.exp(-1j * k * (dirs @ p.pos.T)) * p.area
+        io = p.inout_faces
+        s1, s2, h1, h2 = (np.asarray(getattr(sig, name)) for name in ("sig1", "sig2", "h1", "h2"))
+        if s1.ndim == 1:
+            s1, s2, h1, h2 = s1[:, None], s2[:, None], h1[:, :, None], h2[:, :, None]
+        npol = s1.shape[1]
+        e = np.zeros((len(dirs), 3, npol), dtype=complex)
+        h = np.zeros((len(dirs), 3, npol), dtype=complex)
+        for side, s, hh in ((0, s1, h1), (1, s2, h2)):
+            ind = np.flatnonzero(io[:, side] == self.medium)
+            if len(ind) == 0:
+                continue
+            ph = phase[:, ind]
+            phh = np.einsum("dn,ncp->dcp", ph, hh[ind])
+            phs = ph @ s[ind]
+            e += 1j * k0 * phh - 1j * k * dirs[:, :, None] * phs[:, None, :]
+            h += 1j * k * np.cross(dirs[:, :, None], phh, axis=1)
+        return e, h
+
+    def scattering(self, sig):
+        e, h = self.farfield(sig)
+        dsca = 0.5 * np.real(np.einsum("dc,dcp->dp", self.nvec, np.cross(e, np.conj(h), axis=1)))
+        sca = self.area @ dsca
+        if sca.size == 1:
+            return float(sca[0]), dsca[:, 0]
+        return sca, dsca
+
+
+class PlaneWaveRet:
+    """Plane wave exp(i k dir.r) with polarisation pol (one row per excitation)."""
+
+    def __init__(self, pol, dir, medium=1, pinfty=None, **options):
+        if pol is None or dir is None:
+            raise ValueError("PlaneWaveRet: 'pol' and 'dir' are required")
+        self.pol = np.atleast_2d(np.asarray(pol, dtype=float))
+        self.dir = np.atleast_2d(np.asarray(dir, dtype=float))
+        if self.pol.shape[1] != 3 or self.dir.shape[1] != 3:
+            raise ValueError("PlaneWaveRet: pol and dir must have shape (npol, 3)")
+        self.medium = options.get("medium", medium)
+        self.spec = SpectrumRet(pinfty, medium=self.medium)
+
+    def potential(self, p, enei):
+        """a1, a1p, a2, a2p on the faces touching the embedding medium
+        (planewave_ret.py:257-361)."""
+        if not np.allclose(np.sum(self.pol * self.dir, axis=1), 0):
+            raise ValueError("PlaneWaveRet: polarisation and direction must be orthogonal")
+        eps_val = p.eps[self.medium - 1](enei)[0]
+        k0 = 2 * np.pi / enei
+        k = k0 * np.sqrt(eps_val)
+        npol = self.pol.shape[0]
+        io = p.inout_faces
+        exc = CompStruct(p, enei)
+        for side, name in ((0, "1"), (1, "2")):
+            a = np.zeros((p.n, 3, npol), dtype=complex)
+            ap = np.zeros((p.n, 3, npol), dtype=complex)
+            ind = np.flatnonzero(io[:, side] == self.medium)
+            for i in range(npol):
+                if len(ind):
+                    ph = np.exp(1j * k * p.pos[ind] @ self.dir[i]) / (1j * k0)
+                    a[ind, :, i] = ph[:, None] * self.pol[i]
+                    ap[ind, :, i] = (1j * k * (p.nvec[ind] @ self.dir[i]))[:, None] * ph[:, None] * self.pol[i]
+            if npol == 1:
+                a, ap = a[:, :, 0], ap[:, :, 0]
+            exc.set(**{"a" + name: a, "a" + name + "p": ap})
+        return exc
+
+    __call__ = potential
+
+    def extinction(self, sig):
+        """Optical theorem (planewave_ret.py:437-504)."""
+        e, _ = self.spec.farfield(sig, self.dir)
+        k = complex(np.asarray(sig.p.eps[self.medium - 1](sig.enei)[1]).ravel()[0])
+        npol = self.pol.shape[0]
+        pe = np.array([np.sum(np.conj(self.pol[i]) * e[i, :, i if e.shape[2] > 1 else 0]) for i in range(npol)])
+        ext = np.real(4 * np.pi / k * np.imag(pe))
+        return float(ext[0]) if npol == 1 else ext
+
+    def scattering(self, sig):
+        """(sca, dsca) normalised to the incoming power 0.5 n_b (planewave_ret.py:391-435)."""
+        sca, dsca = self.spec.scattering(sig)
+        nb = np.real(np.sqrt(complex(np.asarray(sig.p.eps[self.medium - 1](sig.enei)[0]).ravel()[0])))
+        return sca / (0.5 * nb), dsca / (0.5 * nb)
+
+    def absorption(self, sig):
+        return self.extinction(sig) - self.scattering(sig)[0]

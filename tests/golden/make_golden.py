@@ -1,0 +1,170 @@
+"""Generate the golden fixtures in this directory from the reference MNPBEM.
+
+Runs the UNMODIFIED reference Python package (import-only stand-ins for its
+absent plotting dependencies are installed by ``_refenv``) and stores small
+input/output vectors that pin the oracle and the geometry module:
+
+* ``geom_spheres.npz``  : face arrays of trisphere(144, 20) and a sample of
+                          trisphere(1444, 40) incl. quadrature points.
+* ``refined_cfg0.npz``  : refinement coefficients (after the closed-surface
+                          correction) of trisphere(144, 20), every 4th entry.
+* ``matrices_s60.npz``  : dense G1, G2, H1, H2 and the solution of
+                          trisphere(32, 10) (60 faces) in water, Drude gold, 600 nm.
+* ``spectrum_cfg0.npz`` : ext / sca of trisphere(144, 20), vacuum, Drude gold,
+                          41 wavelengths 400-800 nm, x-pol along +z.
+* ``dimer_small.npz``   : 2 x trisphere(144, 10), 2 nm gap on x, water, Drude
+                          gold: ext/sca at 3 wavelengths, sig at 620 nm.
+* ``matlab_cfg0.npz``   : MNPBEM17 MATLAB ext/sca/abs of trisphere(144, 20) with
+                          tabulated gold (validation/03_bemret/sphere/data/
+                          bemret_matlab.csv) and the reference EpsTable('gold.dat')
+                          eps at those wavelengths.
+* ``dimer_cfg1.npz``    : ext / sca of the 5768-face dimer (2 x trisphere(1444, 40),
+                          +-21 nm on x, water, Drude gold) at 650 nm, plus
+                          checksums of sig (slow: ~1 min).
+
+Usage:  python tests/golden/make_golden.py [--skip-cfg1]
+"""
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import _refenv  # noqa: E402
+
+_refenv.setup()
+from mnpbem.bem import BEMRet  # noqa: E402
+from mnpbem.geometry import ComParticle, Particle, trisphere  # noqa: E402
+from mnpbem.materials import EpsConst, EpsDrude, EpsTable  # noqa: E402
+from mnpbem.simulation import PlaneWaveRet  # noqa: E402
+
+DRUDE_AU = (9.84, 9.0, 0.067)
+POL = np.array([[1.0, 0.0, 0.0]])
+DIR = np.array([[0.0, 0.0, 1.0]])
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **arrays)
+    print("wrote", name, os.path.getsize(path), "bytes")
+
+
+def geom():
+    out = {}
+    for tag, n, d, sample in (("s144", 144, 20.0, None), ("s1444", 1444, 40.0, np.arange(0, 2884, 97))):
+        p = trisphere(n, d)
+        ind = np.arange(p.nfaces) if sample is None else sample
+        for a in ("pos", "nvec", "tvec1", "tvec2", "area"):
+            out[tag + "_" + a] = getattr(p, a)[ind]
+        out[tag + "_bradius"] = p.bradius()[ind]
+        out[tag + "_ind"] = ind
+        sub = ind[:12]
+        qp, qw, qr = p.quadpol(sub)
+        out[tag + "_quadpol_pos"], out[tag + "_quadpol_w"], out[tag + "_quadpol_row"] = qp, qw, qr
+        qp, qw, qr = Particle.quad(p, sub)
+        out[tag + "_quad_pos"], out[tag + "_quad_w"], out[tag + "_quad_row"] = qp, np.asarray(qw.sum(axis=0)).ravel(), qr
+    save("geom_spheres.npz", **out)
+
+
+def refined_cfg0():
+    p = ComParticle([EpsConst(1.0), EpsDrude(*DRUDE_AU)], [trisphere(144, 20)], [[2, 1]], 1, interp="curv")
+    bem = BEMRet(p)
+    r = bem.g.g[0][0].refined
+    sel = np.arange(0, len(r.row), 4)
+    save("refined_cfg0.npz", row=r.row[sel], col=r.col[sel], g=r.g.real[sel], f=r.f.real[sel],
+         nref=len(r.row), gsum=np.sum(np.abs(r.g)), fsum=np.sum(np.abs(r.f)))
+
+
+def matrices_s60():
+    p = ComParticle([EpsConst(1.77), EpsDrude(*DRUDE_AU)], [trisphere(32, 10)], [[2, 1]], 1, interp="curv")
+    bem = BEMRet(p)
+    enei = 600.0
+    g = bem.g
+    G1 = g.eval(0, 0, "G", enei)
+    G2 = g.eval(1, 1, "G", enei)
+    H1 = g.eval(0, 0, "H1", enei)
+    H2 = g.eval(1, 1, "H2", enei)
+    exc = PlaneWaveRet(POL, DIR)
+    sig, bem = bem.solve(exc.potential(p, enei))
+    save("matrices_s60.npz", enei=enei, G1=G1, G2=G2, H1=H1, H2=H2, sig1=sig.sig1, sig2=sig.sig2,
+         h1=sig.h1, h2=sig.h2, Sigma1=bem.Sigma1, ext=exc.extinction(sig), sca=exc.scattering(sig)[0])
+
+
+def spectrum_cfg0():
+    p = ComParticle([EpsConst(1.0), EpsDrude(*DRUDE_AU)], [trisphere(144, 20)], [[2, 1]], 1, interp="curv")
+    bem = BEMRet(p)
+    exc = PlaneWaveRet(POL, DIR)
+    enei = np.linspace(400, 800, 41)
+    ext = np.zeros(41)
+    sca = np.zeros(41)
+    t0 = time.time()
+    for i, e in enumerate(enei):
+        sig, bem = bem.solve(exc.potential(p, e))
+        ext[i] = exc.extinction(sig)
+        sca[i] = exc.scattering(sig)[0]
+        if i == 20:
+            s20 = sig
+    save("spectrum_cfg0.npz", enei=enei, ext=ext, sca=sca, seconds=time.time() - t0,
+         sig1_600=s20.sig1, sig2_600=s20.sig2, h1_600=s20.h1, h2_600=s20.h2)
+
+
+def _dimer(n, dia, gap_half):
+    a, b = trisphere(n, dia), trisphere(n, dia)
+    a.shift([-(dia / 2 + gap_half), 0, 0])
+    b.shift([dia / 2 + gap_half, 0, 0])
+    return ComParticle([EpsConst(1.77), EpsDrude(*DRUDE_AU)], [a, b], [[2, 1], [2, 1]], 1, 2, interp="curv")
+
+
+def dimer_small():
+    p = _dimer(144, 10.0, 1.0)
+    bem = BEMRet(p)
+    exc = PlaneWaveRet(POL, DIR)
+    enei = np.array([520.0, 620.0, 720.0])
+    ext, sca = [], []
+    for e in enei:
+        sig, bem = bem.solve(exc.potential(p, e))
+        ext.append(exc.extinction(sig))
+        sca.append(exc.scattering(sig)[0])
+        if e == 620.0:
+            s = sig
+    r01 = bem.g.g[0][1].refined
+    save("dimer_small.npz", enei=enei, ext=np.array(ext), sca=np.array(sca), sig1=s.sig1, sig2=s.sig2,
+         h1=s.h1, h2=s.h2, cross_row=r01.row, cross_col=r01.col, cross_g=r01.g.real, cross_f=r01.f.real)
+
+
+def matlab_cfg0():
+    csv = os.path.join(_refenv.REFERENCE_ROOT, "validation", "03_bemret", "sphere", "data", "bemret_matlab.csv")
+    data = np.loadtxt(csv, delimiter=",", skiprows=1)
+    gold = EpsTable("gold.dat")
+    eps = np.array([complex(np.asarray(gold(e)[0]).ravel()[0]) for e in data[:, 0]])
+    save("matlab_cfg0.npz", enei=data[:, 0], ext=data[:, 1], sca=data[:, 2], absorption=data[:, 3], eps_gold=eps)
+
+
+def dimer_cfg1():
+    p = _dimer(1444, 40.0, 1.0)
+    t0 = time.time()
+    bem = BEMRet(p)
+    t1 = time.time()
+    exc = PlaneWaveRet(POL, DIR)
+    sig, bem = bem.solve(exc.potential(p, 650.0))
+    t2 = time.time()
+    ext = exc.extinction(sig)
+    sca = exc.scattering(sig)[0]
+    nref = [len(bem.g.g[i][j].refined.row) for i in range(2) for j in range(2)]
+    save("dimer_cfg1.npz", enei=650.0, ext=ext, sca=sca, nref=np.array(nref),
+         sig1_abs_sum=np.sum(np.abs(sig.sig1)), sig2_abs_sum=np.sum(np.abs(sig.sig2)),
+         h1_abs_sum=np.sum(np.abs(sig.h1)), h2_abs_sum=np.sum(np.abs(sig.h2)),
+         sig2_head=sig.sig2[:64], ctor_s=t1 - t0, solve_s=t2 - t1)
+
+
+if __name__ == "__main__":
+    geom()
+    refined_cfg0()
+    matrices_s60()
+    spectrum_cfg0()
+    dimer_small()
+    matlab_cfg0()
+    if "--skip-cfg1" not in sys.argv:
+        dimer_cfg1()

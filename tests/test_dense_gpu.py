@@ -1,0 +1,90 @@
+"""GPU dense complex LU / solves / GEMM (libbem200) against scipy LAPACK."""
+import ctypes
+
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+from mnpbem_b200 import _native as nat
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand(n, m, seed, dtype=np.complex128):
+    rng = np.random.default_rng(seed)
+    return (rng.standard_normal((n, m)) + 1j * rng.standard_normal((n, m))).astype(dtype)
+
+
+def _t(a):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+
+
+def getrf(A, engine=0):
+    import torch
+    n = A.shape[0]
+    code = nat.C128 if A.dtype == torch.complex128 else nat.C64
+    ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    nat.call("bem200_getrf", code, engine, n, nat.ptr(A), n, nat.ptr(ipiv), nat.ptr(info), None, 0,
+             nat.stream_ptr())
+    return ipiv, info
+
+
+@pytest.mark.parametrize("n", [33, 300, 1100])
+def test_getrf_c128_matches_lapack(cuda, n):
+    A = _rand(n, n, n)
+    At = _t(A)
+    ipiv, info = getrf(At)
+    lu, piv = sla.lu_factor(A)
+    assert int(info.item()) == 0
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv)
+    err = np.max(np.abs(At.cpu().numpy() - lu)) / np.max(np.abs(lu))
+    assert err < 1e-11
+
+
+@pytest.mark.parametrize("n,nrhs", [(300, 1), (700, 5), (1100, 1100)])
+def test_getrs_c128(cuda, n, nrhs):
+    A = _rand(n, n, 7)
+    B = _rand(n, nrhs, 8)
+    At, Bt = _t(A), _t(B)
+    ipiv, _ = getrf(At)
+    nat.call("bem200_getrs", nat.C128, 0, n, nrhs, nat.ptr(At), n, nat.ptr(ipiv), nat.ptr(Bt), nrhs, None, 0,
+             nat.stream_ptr())
+    X = np.linalg.solve(A, B)
+    assert np.max(np.abs(Bt.cpu().numpy() - X)) / np.max(np.abs(X)) < 1e-10
+
+
+def test_getrf_c64(cuda):
+    n = 900
+    A = _rand(n, n, 3)
+    At = _t(A.astype(np.complex64))
+    ipiv, info = getrf(At)
+    B = _rand(n, 4, 4)
+    Bt = _t(B.astype(np.complex64))
+    nat.call("bem200_getrs", nat.C64, 0, n, 4, nat.ptr(At), n, nat.ptr(ipiv), nat.ptr(Bt), 4, None, 0,
+             nat.stream_ptr())
+    X = np.linalg.solve(A, B)
+    assert np.max(np.abs(Bt.cpu().numpy() - X)) / np.max(np.abs(X)) < 1e-3
+
+
+@pytest.mark.parametrize("dt,tol", [(np.complex128, 1e-13), (np.complex64, 1e-5)])
+def test_gemm(cuda, dt, tol):
+    m, n, k = 257, 190, 333
+    A, B, C = _rand(m, k, 1, dt), _rand(k, n, 2, dt), _rand(m, n, 3, dt)
+    At, Bt, Ct = _t(A), _t(B), _t(C)
+    alpha = (ctypes.c_double * 2)(0.5, -1.0)
+    beta = (ctypes.c_double * 2)(1.0, 0.25)
+    code = nat.C128 if dt == np.complex128 else nat.C64
+    nat.call("bem200_gemm", code, 0, m, n, k, alpha, nat.ptr(At), k, nat.ptr(Bt), n, beta, nat.ptr(Ct), n, None, 0,
+             nat.stream_ptr())
+    ref = (0.5 - 1j) * (A.astype(np.complex128) @ B) + (1 + 0.25j) * C
+    assert np.max(np.abs(Ct.cpu().numpy() - ref)) / np.max(np.abs(ref)) < tol
+
+
+def test_singular_pivot_reported(cuda):
+    A = _rand(64, 64, 5)
+    A[:, 10] = 0
+    At = _t(A)
+    _, info = getrf(At)
+    assert int(info.item()) == 11

@@ -1,0 +1,68 @@
+"""Host geometry vs the reference meshes (golden vectors from the reference)."""
+import numpy as np
+
+from conftest import golden
+from mnpbem_b200.geometry import Particle, trisphere
+from mnpbem_b200.quadrature import QuadFace, lgl_nodes
+
+
+def test_quadrature_sums():
+    q = QuadFace()
+    assert len(q.x) == 28 and abs(q.w.sum() - 1) < 1e-14
+    assert len(q.x3) == 144 and abs(q.w3.sum() - 1) < 1e-14
+    assert len(q.x4) == 192 and abs(q.w4.sum() - 4) < 1e-13
+    x, w = lgl_nodes(5)
+    assert abs(w.sum() - 2) < 1e-14 and x[0] == 1.0
+
+
+def test_quadrature_exactness():
+    # the 28-point rule integrates x^a y^b exactly up to degree 11 (sum w = 1 <-> area 1/2)
+    from math import factorial
+    q = QuadFace()
+    for a in range(0, 6):
+        for b in range(0, 6 - a):
+            exact = factorial(a) * factorial(b) / factorial(a + b + 2) * 2  # normalised by area 1/2
+            assert abs(np.sum(q.w * q.x ** a * q.y ** b) - exact) < 1e-13
+
+
+def _cmp(tag, p, g):
+    ind = g[tag + "_ind"]
+    for a in ("pos", "nvec", "tvec1", "tvec2", "area"):
+        np.testing.assert_allclose(getattr(p, a)[ind], g[tag + "_" + a], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(p.bradius()[ind], g[tag + "_bradius"], rtol=0, atol=1e-13)
+    sub = ind[:12]
+    qp, qw, qr = p.quadpol(sub)
+    np.testing.assert_allclose(qp, g[tag + "_quadpol_pos"], atol=1e-13)
+    np.testing.assert_allclose(qw, g[tag + "_quadpol_w"], atol=1e-15)
+    np.testing.assert_array_equal(qr, g[tag + "_quadpol_row"])
+    qp, qw, qr = p.quad_integration(sub)
+    np.testing.assert_allclose(qp, g[tag + "_quad_pos"], atol=1e-13)
+    np.testing.assert_allclose(np.asarray(qw.sum(axis=0)).ravel(), g[tag + "_quad_w"], atol=1e-15)
+
+
+def test_trisphere_matches_reference():
+    g = golden("geom_spheres.npz")
+    _cmp("s144", trisphere(144, 20.0), g)
+    _cmp("s1444", trisphere(1444, 40.0), g)
+
+
+def test_trisphere_topology():
+    p = trisphere(144, 20.0)
+    assert p.nfaces == 284 and p.verts.shape == (144, 3)
+    assert abs(p.area.sum() - np.pi * 20.0 ** 2) / (np.pi * 400) < 2e-3
+    # outward normals
+    assert np.all(np.sum(p.nvec * p.pos, axis=1) > 0)
+
+
+def test_flat_and_quad_faces():
+    # unit cube made of quads: flat areas, centroids and quadrature weights
+    v = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float)
+    f = np.array([[0, 3, 2, 1], [4, 5, 6, 7], [0, 1, 5, 4], [1, 2, 6, 5], [2, 3, 7, 6], [3, 0, 4, 7]], float)
+    p = Particle(v, f)
+    np.testing.assert_allclose(p.area, np.ones(6), atol=1e-14)
+    qp, qw, qr = p.quad_integration()
+    np.testing.assert_allclose(np.asarray(qw.sum(axis=1)).ravel(), np.ones(6), atol=1e-14)
+    pp, pw, pr = p.quadpol()
+    np.testing.assert_allclose(np.bincount(pr, weights=pw), np.ones(6), atol=1e-12)
+    c = p.curved()
+    np.testing.assert_allclose(c.area, np.ones(6), atol=1e-12)

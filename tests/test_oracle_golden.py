@@ -1,0 +1,83 @@
+"""The CPU oracle against golden vectors produced by the reference MNPBEM
+(tests/golden/make_golden.py) and against MNPBEM17 MATLAB results."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from meshes import DRUDE_AU, dimer, rel, sphere
+from mnpbem_b200.geometry import ComParticle, trisphere
+from mnpbem_b200.materials import EpsConst, EpsDrude, EpsValues
+from oracle import green as og
+from oracle.pipeline import OracleBEM
+
+POL = [[1.0, 0, 0]]
+DIR = [[0, 0, 1.0]]
+
+
+def test_refinement_coefficients_cfg0():
+    g = golden("refined_cfg0.npz")
+    cp = sphere()
+    blocks = og.refine_all(cp)
+    b = blocks[0][0]
+    assert len(b.rows) == int(g["nref"])
+    sel = np.arange(0, len(b.rows), 4)
+    np.testing.assert_array_equal(b.rows[sel], g["row"])
+    np.testing.assert_array_equal(b.cols[sel], g["col"])
+    assert rel(b.g[sel], g["g"]) < 1e-13
+    assert rel(b.f[sel], g["f"]) < 1e-13
+
+
+def test_matrices_and_solution_s60():
+    g = golden("matrices_s60.npz")
+    cp = ComParticle([EpsConst(1.77), EpsDrude(*DRUDE_AU)], [trisphere(32, 10.0)], [[2, 1]], 1, interp="curv")
+    ob = OracleBEM(cp)
+    out = ob.solve(float(g["enei"]), POL, DIR, return_state=True)
+    for k in ("G1", "G2", "H1", "H2"):
+        assert rel(out[k], g[k]) < 1e-13, k
+    assert rel(out["state"].Sigma1, g["Sigma1"]) < 1e-11
+    assert rel(out["sig1"][:, 0], g["sig1"]) < 1e-11
+    assert rel(out["h2"][:, :, 0], g["h2"]) < 1e-11
+    assert abs(out["ext"][0] - g["ext"]) / abs(g["ext"]) < 1e-12
+    assert abs(out["sca"][0] - g["sca"]) / abs(g["sca"]) < 1e-12
+
+
+@pytest.mark.slow
+def test_spectrum_cfg0():
+    g = golden("spectrum_cfg0.npz")
+    cp = sphere()
+    ob = OracleBEM(cp)
+    for i in (0, 20, 40):
+        out = ob.solve(float(g["enei"][i]), POL, DIR)
+        assert abs(out["ext"][0] - g["ext"][i]) / g["ext"][i] < 1e-11
+        assert abs(out["sca"][0] - g["sca"][i]) / g["sca"][i] < 1e-11
+        if i == 20:
+            assert rel(out["sig2"][:, 0], g["sig2_600"]) < 1e-11
+            assert rel(out["h1"][:, :, 0], g["h1_600"]) < 1e-11
+
+
+def test_dimer_small():
+    g = golden("dimer_small.npz")
+    cp = dimer()
+    ob = OracleBEM(cp)
+    b01 = ob.blocks[0][1]
+    np.testing.assert_array_equal(b01.rows, g["cross_row"])
+    np.testing.assert_array_equal(b01.cols, g["cross_col"])
+    assert rel(b01.g, g["cross_g"]) < 1e-13 and rel(b01.f, g["cross_f"]) < 1e-13
+    out = ob.solve(620.0, POL, DIR)
+    assert abs(out["ext"][0] - g["ext"][1]) / g["ext"][1] < 1e-11
+    assert abs(out["sca"][0] - g["sca"][1]) / g["sca"][1] < 1e-11
+    assert rel(out["sig1"][:, 0], g["sig1"]) < 1e-10
+
+
+@pytest.mark.slow
+def test_matlab_mnpbem17_tabulated_gold():
+    """trisphere(144, 20), tabulated gold: the oracle reproduces MNPBEM17 (MATLAB)
+    to the 11 digits stored in the reference's validation CSV."""
+    g = golden("matlab_cfg0.npz")
+    table = dict(zip(g["enei"], g["eps_gold"]))
+    cp = ComParticle([EpsConst(1.0), EpsValues(table)], [trisphere(144, 20.0)], [[2, 1]], 1, interp="curv")
+    ob = OracleBEM(cp)
+    for i in range(0, 41, 8):
+        out = ob.solve(float(g["enei"][i]), POL, DIR)
+        assert abs(out["ext"][0] - g["ext"][i]) / g["ext"][i] < 5e-10
+        assert abs(out["sca"][0] - g["sca"][i]) / g["sca"][i] < 5e-10
