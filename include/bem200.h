@@ -45,6 +45,9 @@ extern "C" {
 /* Library version (major * 10000 + minor * 100 + patch). */
 int bem200_version(void);
 
+/* Number of device kernels this library has launched in this process. */
+uint64_t bem200_launch_count(void);
+
 /* Copies the calling thread's last error message into buf (always
  * NUL-terminated when len > 0).  Returns the length of the message. */
 int bem200_last_error(char* buf, size_t len);
@@ -135,13 +138,20 @@ int bem200_gemm(int dtype, int engine, int m, int n, int k, const double* alpha,
                 const void* B, int64_t ldb, const double* beta, void* C, int64_t ldc, void* ws, size_t ws_bytes,
                 void* stream);
 size_t bem200_gemm_workspace_size(int engine, int m, int n, int k);
-/* In-place P A = L U with partial pivoting (largest |re|+|im|); ipiv[k] = row
- * swapped with row k (0-based); *info = first zero pivot (1-based) or 0. */
-int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* ipiv, int32_t* info, void* ws,
-                 size_t ws_bytes, void* stream);
-/* B <- A^-1 B from the getrf factors (nrhs columns, row-major B). */
-int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t ld, const int32_t* ipiv, void* B,
-                 int64_t ldb, void* ws, size_t ws_bytes, void* stream);
+/* In-place P A = L U with partial pivoting (largest |re|+|im|).  Rows are
+ * not moved: logical row i of P A (and of L, U) is storage row rowmap[i].
+ * ipiv[k] = logical row exchanged with row k (LAPACK swap sequence, 0-based);
+ * *info = first exactly-zero pivot (1-based) or 0.  All arrays are device. */
+int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
+                 int32_t* info, void* ws, size_t ws_bytes, void* stream);
+/* B <- A^-1 B from the getrf factors (nrhs columns, row-major B).  scratch:
+ * bem200_getrs_workspace_size bytes.  *status (device int, may be NULL) is set
+ * to BEM200_ERR_TIMEOUT if a bounded device-side wait of the blocked
+ * triangular solve gave up (the result is then invalid). */
+size_t bem200_getrs_workspace_size(int dtype, int n, int nrhs);
+int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t ld, const int32_t* rowmap,
+                 void* B, int64_t ldb, void* ws, size_t ws_bytes, void* scratch, int32_t* status,
+                 void* stream);
 
 /* ------------------------------------------------------------- dense BEM
  * precision 0 = complex128 throughout (the drop-in FP64 path);
@@ -170,6 +180,10 @@ int bem200_bem_solve(int precision, int engine, int n, int npol, void* ws, const
                      const void* alpha, const void* De, int eps_per_face, const double* eps1, const double* eps2,
                      const double* nvec, double k0, void* W1, void* W2, void* scratch, void* gemm_ws,
                      size_t gemm_ws_bytes, void* stream);
+/* Device status of the factors in ws (0 = fine, BEM200_ERR_TIMEOUT = a bounded
+ * wait gave up in the last solve, BEM200_ERR_SINGULAR = zero pivot); copies to
+ * *host_status and synchronises the stream. */
+int bem200_bem_status(int precision, int n, void* ws, int32_t* host_status, void* stream);
 
 /* Full FP64 BEM operator r = A x (b == NULL) or r = b - A x for x = (W1, W2):
  * phi = G1 s1 - G2 s2, a = G1 h1 - G2 h2, alpha = H1 h1 - H2 h2 - ik n (G1 e1 s1

@@ -25,6 +25,7 @@ _sz = ctypes.c_size_t
 # name -> (restype, argtypes)
 _SIGS = {
     "bem200_version": (ctypes.c_int, []),
+    "bem200_launch_count": (ctypes.c_uint64, []),
     "bem200_last_error": (ctypes.c_int, [ctypes.c_char_p, _sz]),
     "bem200_refine_count": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _dbl, _dbl, _vp, _vp]),
     "bem200_scan_i32": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp]),
@@ -41,9 +42,12 @@ _SIGS = {
     "bem200_gemm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                    _i64, _vp, _i64, _vp, _vp, _i64, _vp, _sz, _vp]),
     "bem200_gemm_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
-    "bem200_getrf": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _i64, _vp, _vp, _vp, _sz, _vp]),
+    "bem200_getrf": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _i64, _vp, _vp, _vp, _vp, _sz,
+                                    _vp]),
+    "bem200_getrs_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "bem200_getrs": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _i64, _vp, _vp,
-                                    _i64, _vp, _sz, _vp]),
+                                    _i64, _vp, _sz, _vp, _vp, _vp]),
+    "bem200_bem_status": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "bem200_bem_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int]),
     "bem200_bem_slots": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
     "bem200_bem_init": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp,

@@ -171,26 +171,35 @@ class BEMRet:
     __call__ = init
 
     # --------------------------------------------------------------- solve
-    def solve(self, exc):
-        """Surface charges and currents for excitation ``exc``; returns (sig, self)."""
-        torch = _torch()
+    def rhs(self, exc):
+        """Right-hand side b = [phi | a | alpha | De] (complex128, host) and npol."""
         enei = exc["enei"] if not hasattr(exc, "enei") else exc.enei
-        self.init(enei)
         npol, phi, a, alpha, De = _excitation_rhs(self.p, exc, enei)
-        n = self.n
         b = np.concatenate([phi.reshape(-1), a.reshape(-1), alpha.reshape(-1), De.reshape(-1)])
-        bt = torch.as_tensor(b, dtype=torch.complex128, device=self.dev)
+        return b, npol
+
+    def solve_device(self, bt, npol):
+        """Solve for a device right-hand side ``bt`` (8 n npol complex128); returns
+        device tensors W1 = [sig1 | h1], W2 = [sig2 | h2] (n x 4 npol).  The
+        factors of the current wavelength must be built (``init``)."""
+        torch = _torch()
+        n = self.n
         W1 = torch.empty((n, 4 * npol), dtype=torch.complex128, device=self.dev)
         W2 = torch.empty_like(W1)
         L = nat.lib()
         s = nat.stream_ptr()
-        scratch = torch.empty(int(L.bem200_bem_solve_workspace_size(self._prec, n, npol)), dtype=torch.uint8,
-                              device=self.dev)
+        key = (npol,)
+        if getattr(self, "_scratch_key", None) != key:
+            self._scratch = torch.empty(int(L.bem200_bem_solve_workspace_size(self._prec, n, npol)),
+                                        dtype=torch.uint8, device=self.dev)
+            self._scratch_key = key
+        scratch = self._scratch
         np_ = n * npol
         if self._prec == 0:
+            base = bt.data_ptr()
             nat.call("bem200_bem_solve", 0, 0, n, npol, nat.ptr(self._ws), nat.ptr(bt),
-                     ctypes.c_void_p(bt.data_ptr() + 16 * np_), ctypes.c_void_p(bt.data_ptr() + 16 * 4 * np_),
-                     ctypes.c_void_p(bt.data_ptr() + 16 * 7 * np_), self._eps_mode, self._e1p, self._e2p,
+                     ctypes.c_void_p(base + 16 * np_), ctypes.c_void_p(base + 16 * 4 * np_),
+                     ctypes.c_void_p(base + 16 * 7 * np_), self._eps_mode, self._e1p, self._e2p,
                      nat.ptr(self._nvec), self.k, nat.ptr(W1), nat.ptr(W2), nat.ptr(scratch), nat.ptr(self._gws),
                      self._gws_bytes, s)
         else:
@@ -202,6 +211,29 @@ class BEMRet:
                      nat.ptr(self._nvec), self.k, self.ir_tol, self.ir_maxit, nat.ptr(W1), nat.ptr(W2),
                      nat.ptr(scratch), nat.ptr(self._gws), self._gws_bytes, ctypes.byref(it), ctypes.byref(rr), s)
             self.last_ir = (int(it.value), float(rr.value))
+        return W1, W2
+
+    def check_status(self):
+        """Raise if a factor met a zero pivot or a bounded device wait gave up."""
+        status = ctypes.c_int32(0)
+        nat.call("bem200_bem_status", self._prec, self.n, nat.ptr(self._ws), ctypes.byref(status),
+                 nat.stream_ptr())
+        if status.value != 0:
+            raise RuntimeError("BEMRet: device status {} (3 = zero pivot in a factor, 5 = a bounded device wait "
+                               "gave up)".format(status.value))
+
+    def solve(self, exc):
+        """Surface charges and currents for excitation ``exc``; returns (sig, self)
+        (reference mnpbem/bem/bem_ret.py:1569-1831)."""
+        torch = _torch()
+        enei = exc["enei"] if not hasattr(exc, "enei") else exc.enei
+        self.init(enei)
+        b, npol = self.rhs(exc)
+        n = self.n
+        bt = torch.as_tensor(b, dtype=torch.complex128).to(self.dev, non_blocking=False)
+        W1, W2 = self.solve_device(bt, npol)
+        if self._prec == 0:
+            self.check_status()
         w1 = W1.cpu().numpy()
         w2 = W2.cpu().numpy()
         sig1, h1 = w1[:, :npol], w1[:, npol:].reshape(n, 3, npol)

@@ -25,8 +25,10 @@ template <typename C>
 struct BemState {
   int n;
   C* M[kSlots];
-  int32_t* piv[4];  // G1, G2, Delta, Sigma
+  int32_t* map[4];   // rowmaps of LU(G1), LU(G2), LU(Delta), LU(Sigma)
+  int32_t* ipiv[4];  // LAPACK swap sequences of the same factors
   int* info;
+  int* status;
 };
 
 static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -34,7 +36,7 @@ static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 template <typename C>
 static size_t state_bytes(int n) {
   size_t mat = align256(sizeof(C) * (size_t)n * n);
-  return kSlots * mat + 4 * align256(sizeof(int32_t) * n) + 256;
+  return kSlots * mat + 8 * align256(sizeof(int32_t) * n) + 256;
 }
 
 template <typename C>
@@ -46,10 +48,13 @@ static BemState<C> state_view(int n, void* ws) {
   for (int i = 0; i < kSlots; ++i) s.M[i] = reinterpret_cast<C*>(p + i * mat);
   p += kSlots * mat;
   for (int i = 0; i < 4; ++i) {
-    s.piv[i] = reinterpret_cast<int32_t*>(p);
+    s.map[i] = reinterpret_cast<int32_t*>(p);
+    p += align256(sizeof(int32_t) * n);
+    s.ipiv[i] = reinterpret_cast<int32_t*>(p);
     p += align256(sizeof(int32_t) * n);
   }
   s.info = reinterpret_cast<int*>(p);
+  s.status = s.info + 1;
   return s;
 }
 
@@ -102,23 +107,24 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
   const long long nn = (long long)n * n;
   LaContext c = ctx;
   c.dinfo = s.info;
-  BEM_CUDA_CHECK(cudaMemsetAsync(s.info, 0, sizeof(int), ctx.stream));
+  c.dstatus = s.status;
+  BEM_CUDA_CHECK(cudaMemsetAsync(s.info, 0, 2 * sizeof(int), ctx.stream));
   int st;
   // LU(G1), LU(G2)
-  if ((st = getrf<C>(c, n, s.M[0], n, s.piv[0]))) return st;
-  if ((st = getrf<C>(c, n, s.M[1], n, s.piv[1]))) return st;
+  if ((st = getrf<C>(c, n, s.M[0], n, s.map[0], s.ipiv[0], nullptr))) return st;
+  if ((st = getrf<C>(c, n, s.M[1], n, s.map[1], s.ipiv[1], nullptr))) return st;
   // Sigma1 = H1 G1^-1, Sigma2 = H2 G2^-1 (right solves; M5 is scratch)
-  if ((st = solve_right<C>(c, n, n, s.M[0], n, s.piv[0], s.M[2], n, s.M[5]))) return st;
-  if ((st = solve_right<C>(c, n, n, s.M[1], n, s.piv[1], s.M[3], n, s.M[5]))) return st;
+  if ((st = solve_right<C>(c, n, n, s.M[0], n, s.map[0], s.M[2], n, s.M[5]))) return st;
+  if ((st = solve_right<C>(c, n, n, s.M[1], n, s.map[1], s.M[3], n, s.M[5]))) return st;
   // Delta = Sigma1 - Sigma2, LU(Delta), Delta^-1
   delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[4]);
   BEM_LAUNCH_CHECK();
-  if ((st = getrf<C>(c, n, s.M[4], n, s.piv[2]))) return st;
-  if ((st = inverse<C>(c, n, s.M[4], n, s.piv[2], s.M[5], n))) return st;
+  if ((st = getrf<C>(c, n, s.M[4], n, s.map[2], s.ipiv[2], nullptr))) return st;
+  if ((st = inverse<C>(c, n, s.M[4], n, s.map[2], s.M[5], n))) return st;
   // Sigma, LU(Sigma)
   sigma_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(n, s.M[2], s.M[3], s.M[5], nvec, eps, k0 * k0, s.M[6]);
   BEM_LAUNCH_CHECK();
-  if ((st = getrf<C>(c, n, s.M[6], n, s.piv[3]))) return st;
+  if ((st = getrf<C>(c, n, s.M[6], n, s.map[3], s.ipiv[3], nullptr))) return st;
   return BEM200_OK;
 }
 
@@ -230,16 +236,19 @@ __global__ void solve_pack_kernel(int n, int p, const C* __restrict__ sig2, cons
 }
 
 template <typename C>
-static size_t solve_scratch_elems(int n, int p) {
-  return (size_t)n * p * 20;
+static size_t solve_scratch_bytes(int n, int p) {
+  return align256(sizeof(C) * (size_t)n * p * 20) + align256(solve_left_scratch_bytes<C>(n, 4 * p));
 }
 
 // Solve for (W1 = [sig1 | h1], W2 = [sig2 | h2]) given RHS (phi, a, alpha, De)
-// in element type C.  scratch: solve_scratch_elems elements of C.
+// in element type C.  scratch: solve_scratch_bytes.
 template <typename C>
-static int bem_solve_core(const LaContext& ctx, int n, int p, void* ws, const C* phi, const C* a, const C* alpha,
+static int bem_solve_core(const LaContext& ctx0, int n, int p, void* ws, const C* phi, const C* a, const C* alpha,
                           const C* De, const EpsArg& eps, const double* nvec, double k0, C* W1, C* W2, C* scratch) {
   BemState<C> s = state_view<C>(n, ws);
+  LaContext ctx = ctx0;
+  ctx.dstatus = s.status;
+  void* lscr = reinterpret_cast<char*>(scratch) + align256(sizeof(C) * (size_t)n * p * 20);
   cudaStream_t st_ = ctx.stream;
   const long long np = (long long)n * p;
   C* T = scratch;             // n x 4p
@@ -261,15 +270,15 @@ static int bem_solve_core(const LaContext& ctx, int n, int p, void* ws, const C*
   solve_rhs_sig_kernel<C><<<ceil_div(np, 256), 256, 0, st_>>>(n, p, Dm, X, nvec, eps, k0, rs);
   BEM_LAUNCH_CHECK();
   // sig2 = Sigma^-1 rs   (in place in rs)
-  if ((st = solve_left<C>(ctx, n, p, s.M[6], n, s.piv[3], rs, p))) return st;
+  if ((st = solve_left<C>(ctx, n, p, s.M[6], n, s.map[3], rs, p, lscr))) return st;
   // h2 = Delta^-1 (ik n L sig2 + Am)
   solve_rhs_h_kernel<C><<<ceil_div(3 * np, 256), 256, 0, st_>>>(n, p, rs, Am, nvec, eps, k0, X);
   BEM_LAUNCH_CHECK();
   if ((st = gemm<C>(ctx, n, 3 * p, n, one, s.M[5], n, X, 3 * p, zero, h2, 3 * p))) return st;
   solve_pack_kernel<C><<<ceil_div(4 * np, 256), 256, 0, st_>>>(n, p, rs, h2, phi, a, W1, W2);
   BEM_LAUNCH_CHECK();
-  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[0], n, s.piv[0], W1, 4 * p))) return st;
-  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[1], n, s.piv[1], W2, 4 * p))) return st;
+  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[0], n, s.map[0], W1, 4 * p, lscr))) return st;
+  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[1], n, s.map[1], W2, 4 * p, lscr))) return st;
   return BEM200_OK;
 }
 
@@ -455,9 +464,10 @@ int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face
 
 size_t bem200_bem_solve_workspace_size(int precision, int n, int npol) {
   size_t np = (size_t)n * npol;
-  if (precision == 0) return sizeof(double2) * 20 * np;
+  if (precision == 0) return solve_scratch_bytes<double2>(n, npol);
   // mixed: c64 core scratch + c64 rhs/solution + c128 IR vectors + operator scratch
-  return sizeof(float2) * (20 * np + 16 * np) + sizeof(double2) * (8 * np * 3 + 40 * np) + 256;
+  return align256(solve_scratch_bytes<float2>(n, npol)) + 2 * align256(sizeof(float2) * 8 * np) +
+         2 * align256(sizeof(double2) * 8 * np) + align256(sizeof(double2) * 40 * np) + 256;
 }
 
 int bem200_bem_solve(int precision, int engine, int n, int npol, void* ws, const void* phi, const void* a,
@@ -475,6 +485,16 @@ int bem200_bem_solve(int precision, int engine, int n, int npol, void* ws, const
   EpsArg eps = make_eps(eps_per_face, eps1, eps2);
   return bem_solve_core<double2>(ctx, n, npol, ws, (const double2*)phi, (const double2*)a, (const double2*)alpha,
                                  (const double2*)De, eps, nvec, k0, (double2*)W1, (double2*)W2, (double2*)scratch);
+}
+
+int bem200_bem_status(int precision, int n, void* ws, int32_t* host_status, void* stream) {
+  BEM_REQUIRE(ws && host_status && n > 0, BEM200_ERR_ARG, "bem_status: bad arguments");
+  int* info = precision == 0 ? state_view<double2>(n, ws).info : state_view<float2>(n, ws).info;
+  int h[2] = {0, 0};
+  BEM_CUDA_CHECK(cudaMemcpyAsync(h, info, 2 * sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  BEM_CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
+  *host_status = h[1] ? h[1] : (h[0] ? BEM200_ERR_SINGULAR : 0);
+  return BEM200_OK;
 }
 
 int bem200_bem_apply(int n, int npol, const void* G1, const void* G2, const void* H1, const void* H2,
@@ -514,14 +534,14 @@ int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, c
   ctx.ws_bytes = gemm_ws_bytes;
   EpsArg eps = make_eps(eps_per_face, eps1, eps2);
   const long long np = (long long)n * npol;
+  // every sub-buffer starts on a 256-byte boundary
   char* p = reinterpret_cast<char*>(scratch);
-  float2* core = reinterpret_cast<float2*>(p);        p += sizeof(float2) * 20 * np;
-  float2* rhs32 = reinterpret_cast<float2*>(p);       p += sizeof(float2) * 8 * np;
-  float2* sol32 = reinterpret_cast<float2*>(p);       p += sizeof(float2) * 8 * np;
-  double2* r = reinterpret_cast<double2*>(p);         p += sizeof(double2) * 8 * np;
-  double2* x = reinterpret_cast<double2*>(p);         p += sizeof(double2) * 8 * np;
-  p += sizeof(double2) * 8 * np;  // reserved
-  double2* opws = reinterpret_cast<double2*>(p);      p += sizeof(double2) * 40 * np;
+  float2* core = reinterpret_cast<float2*>(p);        p += align256(solve_scratch_bytes<float2>(n, npol));
+  float2* rhs32 = reinterpret_cast<float2*>(p);       p += align256(sizeof(float2) * 8 * np);
+  float2* sol32 = reinterpret_cast<float2*>(p);       p += align256(sizeof(float2) * 8 * np);
+  double2* r = reinterpret_cast<double2*>(p);         p += align256(sizeof(double2) * 8 * np);
+  double2* x = reinterpret_cast<double2*>(p);         p += align256(sizeof(double2) * 8 * np);
+  double2* opws = reinterpret_cast<double2*>(p);      p += align256(sizeof(double2) * 40 * np);
   unsigned long long* red = reinterpret_cast<unsigned long long*>(p);
   cudaStream_t s = ctx.stream;
   const double2* bb = (const double2*)b;
@@ -550,6 +570,12 @@ int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, c
                         eps, nvec, k0, x, x + 4 * np, bb, r, opws)))
       return st;
     if ((st = absmax_host(s, 8 * np, r, red, &rnorm))) return st;
+    {
+      int hs = 0;
+      BEM_CUDA_CHECK(cudaMemcpyAsync(&hs, state_view<float2>(n, ws).status, sizeof(int), cudaMemcpyDeviceToHost, s));
+      BEM_CUDA_CHECK(cudaStreamSynchronize(s));
+      BEM_REQUIRE(hs == 0, BEM200_ERR_TIMEOUT, "bem_solve_ir: a bounded device wait gave up (status %d)", hs);
+    }
     ++it;
     if (!(rnorm <= tol * bnorm) && !(rnorm < 1e300)) break;  // NaN / overflow: stop
     if (rnorm <= tol * bnorm || it >= maxit) break;

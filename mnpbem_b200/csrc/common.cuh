@@ -25,7 +25,14 @@ const char* get_error();
     }                                                                             \
   } while (0)
 
-#define BEM_LAUNCH_CHECK() BEM_CUDA_CHECK(cudaGetLastError())
+// Kernel launches are counted (bem200_launch_count) so that callers can report
+// how many device kernels a call enqueued.
+void count_launch();
+#define BEM_LAUNCH_CHECK()          \
+  do {                              \
+    ::bem200::count_launch();       \
+    BEM_CUDA_CHECK(cudaGetLastError()); \
+  } while (0)
 
 #define BEM_REQUIRE(cond, code, ...)                                              \
   do {                                                                            \
@@ -98,6 +105,16 @@ template <> __host__ __device__ __forceinline__ float2 cmake<float2>(double re, 
   return make_float2((float)re, (float)im);
 }
 
-inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+__host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Kernel attributes are set once per kernel (the call is a host-side round
+// trip that should not sit in front of every launch).  Entries are keyed by
+// the kernel's address; a larger shared-memory request raises the limit again.
+cudaError_t set_kernel_attrs(const void* kern, int smem_bytes, bool nonportable_cluster);
+
+template <typename K>
+inline cudaError_t set_kernel_attrs_once(K kern, int smem_bytes, bool nonportable_cluster) {
+  return set_kernel_attrs(reinterpret_cast<const void*>(kern), smem_bytes, nonportable_cluster);
+}
 
 }  // namespace bem200

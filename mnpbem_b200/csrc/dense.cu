@@ -1,18 +1,20 @@
 // Dense complex LU with partial pivoting, triangular solves and GEMM.
 //
-// Structure (all host-driven, kernels enqueued on one stream):
-//   * recursive LU: the leaf panel (width <= kPanelNB) is factored by ONE
-//     thread-block cluster that keeps the whole tall panel in distributed
-//     shared memory; per column, the pivot search and the row exchange use
-//     DSMEM and two cluster barriers.  The rest of the work is TRSM + GEMM.
-//   * recursive TRSM with small substitution kernels at the leaves.
-//   * GEMM: CUDA-core kernel for complex128 (FP64 FMA) / complex64 (FP32),
-//     and the tcgen05 tensor-core path for complex64 (gemm_tc.cu).
-// Pivot choice follows LAPACK izamax: largest |re| + |im|, first index on ties.
+// Structure (host-driven recursion, kernels enqueued on one stream):
+//   * recursive LU; the leaf panel (width <= 32) is factored by ONE
+//     thread-block cluster that keeps the tall panel in distributed shared
+//     memory.  Pivoting is lazy: rows stay where they are and a rowmap
+//     (logical -> storage row) is updated, so there are no row-swap passes;
+//     each column costs one cluster barrier (candidates are double buffered).
+//   * recursive TRSM with small substitution kernels at the leaves, and a
+//     blocked triangular solve for few right-hand sides in which row blocks
+//     wait on flags of the blocks they depend on (bounded waits).
+//   * GEMM on row views: CUDA-core kernel for complex128 (FP64 FMA) /
+//     complex64, and the tcgen05 tensor-core path for complex64 (gemm_tc.cu).
+// Pivot choice follows LAPACK izamax: largest |re| + |im|.
 #include <cooperative_groups.h>
 
 #include <climits>
-#include <vector>
 
 #include "dense.cuh"
 
@@ -25,33 +27,52 @@ template <typename C> using R_t = typename cplx_traits<C>::real;
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
 __device__ __forceinline__ float cabs1(float2 a) { return fabsf(a.x) + fabsf(a.y); }
 
+template <typename C>
+__device__ __forceinline__ C shfl_c(C v, int src) {
+  v.x = __shfl_sync(0xffffffffu, v.x, src);
+  v.y = __shfl_sync(0xffffffffu, v.y, src);
+  return v;
+}
+
 // ===================================================================== GEMM
-// C = alpha A B + beta C; block tile 64 x 64, each thread a 4 x 4 register tile
-// (rows ty + 16 i, cols tx + 16 j).
+// C = alpha A B + beta C on row views; block tile 64 x 64, each thread a 4 x 4
+// register tile (rows ty + 16 i, cols tx + 16 j).
 template <typename C, int BK>
-__global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C alpha, const C* __restrict__ A,
-                                                        long long lda, const C* __restrict__ B, long long ldb,
-                                                        C beta, C* __restrict__ Cm, long long ldc) {
+__global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C alpha, RowView<C> A, RowView<C> B,
+                                                        C beta, RowView<C> Cv) {
   constexpr int BM = 64, BN = 64;
+  constexpr int A_LOADS = BM * BK / 256;  // rows of A loaded per thread (fixed over k)
+  constexpr int B_LOADS = BK * BN / 256;
   __shared__ C As[BK][BM + 1];
   __shared__ C Bs[BK][BN];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  // this thread loads A rows ar0 + i * (256 / BK), column ac of each k-slab
+  const int ac = tid % BK, ar0 = tid / BK;
+  long long aoff[A_LOADS];
+#pragma unroll
+  for (int i = 0; i < A_LOADS; ++i) {
+    int gr = m0 + ar0 + i * (256 / BK);
+    aoff[i] = gr < m ? A.off(gr, 0) : -1;
+  }
+  const int bc = tid % BN, br0 = tid / BN;
+  const bool bcol_ok = (n0 + bc) < n;
   C acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = czero<C>();
   for (int k0 = 0; k0 < k; k0 += BK) {
-    for (int idx = threadIdx.x; idx < BM * BK; idx += 256) {
-      int r = idx / BK, c = idx % BK;
-      int gr = m0 + r, gc = k0 + c;
-      As[c][r] = (gr < m && gc < k) ? A[(long long)gr * lda + gc] : czero<C>();
-    }
-    for (int idx = threadIdx.x; idx < BK * BN; idx += 256) {
-      int r = idx / BN, c = idx % BN;
-      int gr = k0 + r, gc = n0 + c;
-      Bs[r][c] = (gr < k && gc < n) ? B[(long long)gr * ldb + gc] : czero<C>();
+    const bool kfull = (k0 + BK) <= k;
+    const int gc = k0 + ac;
+#pragma unroll
+    for (int i = 0; i < A_LOADS; ++i)
+      As[ac][ar0 + i * (256 / BK)] = (aoff[i] >= 0 && (kfull || gc < k)) ? A.base[aoff[i] + gc] : czero<C>();
+#pragma unroll
+    for (int i = 0; i < B_LOADS; ++i) {
+      int gr = k0 + br0 + i * (256 / BN);
+      Bs[br0 + i * (256 / BN)][bc] = (gr < k && bcol_ok) ? B.at(gr, n0 + bc) : czero<C>();
     }
     __syncthreads();
 #pragma unroll
@@ -78,262 +99,468 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C a
   for (int i = 0; i < 4; ++i) {
     int gr = m0 + ty + 16 * i;
     if (gr >= m) continue;
+    const long long roff = Cv.off(gr, 0);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       int gc = n0 + tx + 16 * j;
       if (gc >= n) continue;
       C v = cmul(alpha, acc[i][j]);
-      long long o = (long long)gr * ldc + gc;
-      if (use_beta) v = cadd(v, cmul(beta, Cm[o]));
-      Cm[o] = v;
+      C& out = Cv.base[roff + gc];
+      if (use_beta) v = cadd(v, cmul(beta, out));
+      out = v;
     }
   }
 }
 
 template <typename C>
-int gemm(const LaContext& ctx, int m, int n, int k, C alpha, const C* A, long long lda, const C* B, long long ldb,
-         C beta, C* Cm, long long ldc) {
+int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv) {
   if (m <= 0 || n <= 0) return BEM200_OK;
-  if (k <= 0) {
-    // C = beta C: run the kernel with k = 0 (acc = 0)
+  if constexpr (sizeof(C) == 8) {
+    if (ctx.engine != GemmEngine::kSimt && k >= 64 && m >= 128 && n >= 64)
+      return gemm_tc_c64(ctx, m, n, k, alpha, A, B, beta, Cv);
   }
   dim3 grid(ceil_div(n, 64), ceil_div(m, 64));
   BEM_REQUIRE(grid.y <= 65535, BEM200_ERR_ARG, "gemm: m too large");
   constexpr int BK = sizeof(C) == 16 ? 8 : 16;
-  gemm_simt_kernel<C, BK><<<grid, 256, 0, ctx.stream>>>(m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc);
+  gemm_simt_kernel<C, BK><<<grid, 256, 0, ctx.stream>>>(m, n, k, alpha, A, B, beta, Cv);
   BEM_LAUNCH_CHECK();
   return BEM200_OK;
-}
-
-template <>
-int gemm<float2>(const LaContext& ctx, int m, int n, int k, float2 alpha, const float2* A, long long lda,
-                 const float2* B, long long ldb, float2 beta, float2* Cm, long long ldc) {
-  if (m <= 0 || n <= 0) return BEM200_OK;
-  if (ctx.engine != GemmEngine::kSimt && k >= 64 && m >= 128 && n >= 64)
-    return gemm_tc_c64(ctx, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc);
-  dim3 grid(ceil_div(n, 64), ceil_div(m, 64));
-  BEM_REQUIRE(grid.y <= 65535, BEM200_ERR_ARG, "gemm: m too large");
-  gemm_simt_kernel<float2, 16><<<grid, 256, 0, ctx.stream>>>(m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc);
-  BEM_LAUNCH_CHECK();
-  return BEM200_OK;
-}
-
-// ===================================================================== row swaps
-// for kk in [k0, k1) (forward) swap rows kk and ipiv[kk] over columns [c0, c1)
-template <typename C>
-__global__ void laswp_kernel(C* A, long long ld, int c0, int c1, const int32_t* __restrict__ ipiv, int k0, int k1) {
-  int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= c1) return;
-  for (int kk = k0; kk < k1; ++kk) {
-    int p = ipiv[kk];
-    if (p != kk) {
-      C t = A[(long long)kk * ld + c];
-      A[(long long)kk * ld + c] = A[(long long)p * ld + c];
-      A[(long long)p * ld + c] = t;
-    }
-  }
-}
-
-template <typename C>
-static int laswp(const LaContext& ctx, C* A, long long ld, int c0, int c1, const int32_t* ipiv, int k0, int k1) {
-  if (c1 <= c0 || k1 <= k0) return BEM200_OK;
-  laswp_kernel<C><<<ceil_div(c1 - c0, 128), 128, 0, ctx.stream>>>(A, ld, c0, c1, ipiv, k0, k1);
-  BEM_LAUNCH_CHECK();
-  return BEM200_OK;
-}
-
-// permutation of the swaps: perm[i] = original row now at position i
-__global__ void ipiv_to_perm_kernel(int n, const int32_t* __restrict__ ipiv, int32_t* __restrict__ perm) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int i = 0; i < n; ++i) perm[i] = i;
-  for (int kk = 0; kk < n; ++kk) {
-    int p = ipiv[kk];
-    int t = perm[kk];
-    perm[kk] = perm[p];
-    perm[p] = t;
-  }
-}
-
-// Y[r, perm[i]] = X[r, i]   (X P for the row-permutation matrix P of the swaps)
-template <typename C>
-__global__ void colperm_kernel(int m, int n, const C* __restrict__ X, long long ldx, const int32_t* __restrict__ perm,
-                               C* __restrict__ Y, long long ldy) {
-  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long long)m * n) return;
-  int r = (int)(idx / n), i = (int)(idx % n);
-  Y[(long long)r * ldy + perm[i]] = X[(long long)r * ldx + i];
 }
 
 // ===================================================================== panel LU
-// Factor rows [col0, n) x columns [col0, col0 + w) with partial pivoting.
-// One cluster of `cs` CTAs; CTA `rank` keeps panel rows [rank*R, rank*R + R)
-// in shared memory.  ipiv[col0 + t] = global pivot row of step t.
+// Factor logical rows [0, m) x columns [0, w) of view (map, col) with partial
+// pivoting and no row movement.  The cluster's CTA `rank` keeps panel rows
+// [rank R, rank R + R) in shared memory; warp w owns rows r = w (mod 8) and
+// lane c owns panel column c.
 constexpr int kPanelNB = 32;
-constexpr int kPanelThreads = 256;
+constexpr int kPanelWarps = 16;
+constexpr int kPanelThreads = 32 * kPanelWarps;
+constexpr int kPanelUnroll = 4;
 
 template <typename C>
 struct PanelShared {
-  R_t<C> red_val[kPanelThreads / 32];
-  int red_row[kPanelThreads / 32];
-  R_t<C> cand_val;
-  int cand_row;
-  int piv_row;
+  R_t<C> wval[kPanelWarps];        // per-warp candidates of the current column
+  int wrow[kPanelWarps];
+  R_t<C> cval[2];                  // this CTA's published candidate (double buffered)
+  int crow[2];
+  C crowdata[2][kPanelNB];         // ... and its row
+  int p;                           // pivot (panel row) of the current column
+  C prow[kPanelNB];                // pivot row of the current column
+  int perm[kPanelNB];
   int singular;
-  C prow[kPanelNB];
-  C trow[kPanelNB];
+  int mk[2 * kPanelNB];
+  int mv[2 * kPanelNB];
+  int mo[2 * kPanelNB];
 };
 
+// pivot magnitude; NaN counts as 0 so that every unused row stays selectable
+__device__ __forceinline__ double pmag(double2 a) {
+  double v = fabs(a.x) + fabs(a.y);
+  return v >= 0 ? v : 0.0;
+}
+__device__ __forceinline__ float pmag(float2 a) {
+  float v = fabsf(a.x) + fabsf(a.y);
+  return v >= 0 ? v : 0.f;
+}
+
 template <typename C>
-__global__ void __launch_bounds__(kPanelThreads) panel_lu_kernel(int n, int col0, int w, C* __restrict__ A,
-                                                                 long long ld, int32_t* __restrict__ ipiv,
+__device__ __forceinline__ void cand_merge(R_t<C>& b, int& br, R_t<C> v, int rw) {
+  if (v > b || (v == b && rw < br)) {
+    b = v;
+    br = rw;
+  }
+}
+
+
+// Replay the panel's pivot sequence perm[0..w) (panel rows) as LAPACK row
+// swaps on a position map with <= 2w entries held in the registers of one
+// warp (two slots per lane), write ipiv, and move the rowmap entries of the
+// swapped positions.  Called by a full warp.
+__device__ void replay_pivots(int w, const int* __restrict__ perm, int32_t* __restrict__ ipiv, int ipiv_base,
+                              int32_t* __restrict__ rowmap) {
+  const int lane = threadIdx.x & 31;
+  int key[2] = {-1, -1}, val[2] = {-1, -1};
+  int nmap = 0;
+  auto find = [&](const int (&arr)[2], int x, int& slot) -> bool {
+    unsigned m0 = __ballot_sync(0xffffffffu, arr[0] == x);
+    unsigned m1 = __ballot_sync(0xffffffffu, arr[1] == x);
+    if (m0) { slot = __ffs(m0) - 1; return true; }
+    if (m1) { slot = 32 + __ffs(m1) - 1; return true; }
+    return false;
+  };
+  auto get = [&](const int (&arr)[2], int slot) -> int {
+    return __shfl_sync(0xffffffffu, slot < 32 ? arr[0] : arr[1], slot & 31);
+  };
+  auto put = [&](int pos, int prow) {
+    int slot;
+    if (!find(key, pos, slot)) {
+      slot = nmap++;
+      if (lane == (slot & 31)) key[slot >> 5] = pos;
+    }
+    if (lane == (slot & 31)) val[slot >> 5] = prow;
+  };
+  for (int t = 0; t < w; ++t) {
+    const int q = perm[t];
+    int slot;
+    const int pp = find(val, q, slot) ? get(key, slot) : q;     // current position of panel row q
+    const int at_t = find(key, t, slot) ? get(val, slot) : t;   // panel row at position t
+    put(t, q);
+    put(pp, at_t);
+    if (lane == 0) ipiv[t] = ipiv_base + pp;
+  }
+  // new rowmap[pos] = old rowmap[panel row now at pos]
+  int mo[2];
+  for (int k = 0; k < 2; ++k) mo[k] = (key[k] >= 0) ? rowmap[val[k]] : 0;
+  __syncwarp();
+  for (int k = 0; k < 2; ++k)
+    if (key[k] >= 0) rowmap[key[k]] = mo[k];
+}
+
+template <typename C>
+__device__ __forceinline__ void warp_argmax(R_t<C>& b, int& br) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    cand_merge<C>(b, br, __shfl_xor_sync(0xffffffffu, b, o), __shfl_xor_sync(0xffffffffu, br, o));
+}
+
+// Per column: warps publish candidates in shared memory; warp 0 reduces them,
+// publishes the CTA's best row, and after ONE cluster barrier gathers the
+// cs candidates (one remote load per lane) and the winning row (one more
+// remote load per lane); everyone else reads the result from local shared
+// memory.  Published slots are double buffered: a slot is rewritten two
+// columns later, after every CTA has passed the next barrier.
+template <typename C>
+__global__ void __launch_bounds__(kPanelThreads) panel_lu_kernel(int m, int w, C* __restrict__ A, long long ld,
+                                                                 int col, int32_t* __restrict__ rowmap,
+                                                                 int32_t* __restrict__ ipiv, int ipiv_base,
                                                                  int* __restrict__ info, int R) {
   using Real = R_t<C>;
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
   const int rank = (int)cluster.block_rank();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* rows = reinterpret_cast<C*>(smem_raw);  // R x kPanelNB
+  C* rows = reinterpret_cast<C*>(smem_raw);                                   // R x 32
+  int32_t* phys = reinterpret_cast<int32_t*>(rows + (size_t)R * kPanelNB);    // R
+  uint8_t* used = reinterpret_cast<uint8_t*>(phys + R);                       // R
   __shared__ PanelShared<C> sh;
-  const int m = n - col0;
   const int r0 = rank * R;
   const int rcount = max(0, min(R, m - r0));
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
+  for (int r = tid; r < rcount; r += kPanelThreads) {
+    phys[r] = rowmap[r0 + r];
+    used[r] = 0;
+  }
+  __syncthreads();
   for (int idx = tid; idx < rcount * kPanelNB; idx += kPanelThreads) {
-    int r = idx / kPanelNB, c = idx % kPanelNB;
-    rows[idx] = (c < w) ? A[(long long)(col0 + r0 + r) * ld + col0 + c] : czero<C>();
+    int r = idx >> 5, c = idx & 31;
+    rows[idx] = (c < w) ? A[(long long)phys[r] * ld + col + c] : czero<C>();
   }
   if (tid == 0) sh.singular = 0;
   __syncthreads();
 
+  // candidates for column 0
+  Real best = -1;
+  int brow = INT_MAX;
+  for (int r = wid + kPanelWarps * lane; r < rcount; r += 32 * kPanelWarps)
+    cand_merge<C>(best, brow, pmag(rows[r * kPanelNB]), r);
+  warp_argmax<C>(best, brow);
+
   for (int t = 0; t < w; ++t) {
-    // ---- local candidate: max |re|+|im| in column t over panel rows >= t
-    Real best = -1;
-    int brow = INT_MAX;
-    for (int r = tid; r < rcount; r += kPanelThreads) {
-      int pr = r0 + r;
-      if (pr < t) continue;
-      Real a = cabs1(rows[r * kPanelNB + t]);
-      if (a > best || (a == best && pr < brow)) {
-        best = a;
-        brow = pr;
-      }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      Real ov = __shfl_xor_sync(0xffffffffu, best, o);
-      int orw = __shfl_xor_sync(0xffffffffu, brow, o);
-      if (ov > best || (ov == best && orw < brow)) {
-        best = ov;
-        brow = orw;
-      }
-    }
+    const int buf = t & 1;
     if (lane == 0) {
-      sh.red_val[wid] = best;
-      sh.red_row[wid] = brow;
+      sh.wval[wid] = best;
+      sh.wrow[wid] = brow;  // local row index
     }
     __syncthreads();
-    if (tid == 0) {
-      Real b = sh.red_val[0];
-      int br = sh.red_row[0];
-      for (int q = 1; q < kPanelThreads / 32; ++q) {
-        if (sh.red_val[q] > b || (sh.red_val[q] == b && sh.red_row[q] < br)) {
-          b = sh.red_val[q];
-          br = sh.red_row[q];
-        }
+    if (wid == 0) {
+      Real b = lane < kPanelWarps ? sh.wval[lane] : (Real)-1;
+      int br = lane < kPanelWarps ? sh.wrow[lane] : INT_MAX;
+      warp_argmax<C>(b, br);
+      sh.crowdata[buf][lane] = (br < rcount) ? rows[br * kPanelNB + lane] : czero<C>();
+      if (lane == 0) {
+        sh.cval[buf] = (br < rcount) ? b : (Real)-1;
+        sh.crow[buf] = (br < rcount) ? r0 + br : INT_MAX;
       }
-      sh.cand_val = b;
-      sh.cand_row = br;
     }
-    cluster.sync();  // candidates of all CTAs visible
+    if (cs > 1) cluster.sync(); else __syncthreads();
     if (wid == 0) {
       Real b = -1;
       int br = INT_MAX;
       if (lane < cs) {
-        PanelShared<C>* rs = cluster.map_shared_rank(&sh, lane);
-        b = rs->cand_val;
-        br = rs->cand_row;
+        const PanelShared<C>* rs = (cs > 1) ? cluster.map_shared_rank(&sh, lane) : &sh;
+        b = rs->cval[buf];
+        br = rs->crow[buf];
+      }
+      warp_argmax<C>(b, br);
+      // every step has an unused row, each with magnitude >= 0 > -1: br < m
+      const int p = min(br, m - 1);
+      const int owner = p / R;
+      const PanelShared<C>* os = (cs > 1) ? cluster.map_shared_rank(&sh, owner) : &sh;
+      sh.prow[lane] = os->crowdata[buf][lane];
+      if (lane == 0) {
+        sh.p = p;
+        sh.perm[t] = p;
+        if (!(b > 0) && !sh.singular) sh.singular = t + 1;
+      }
+    }
+    __syncthreads();
+    const int p = sh.p;
+    const int owner = p / R, lr = p - owner * R;
+    const C pc = sh.prow[lane];
+    const C piv = shfl_c(pc, t);
+    const bool ok = cabs1(piv) > 0;
+    // multipliers use the reciprocal of the pivot, as LAPACK's scaling does
+    const C inv = ok ? cdiv(cmake<C>(1.0, 0.0), piv) : czero<C>();
+    // update the unused rows owned by this warp (kPanelUnroll rows in flight,
+    // straight-line selects); track candidates for column t + 1
+    best = -1;
+    brow = INT_MAX;
+    const bool at_t = lane == t, after_t = lane > t, next_t = lane == t + 1;
+    for (int rb = wid; rb < rcount; rb += kPanelWarps * kPanelUnroll) {
+      C v[kPanelUnroll];
+      bool act[kPanelUnroll];
+      int rr[kPanelUnroll];
+#pragma unroll
+      for (int u = 0; u < kPanelUnroll; ++u) {
+        const int r = rb + u * kPanelWarps;
+        const bool in = r < rcount;
+        rr[u] = in ? r : rb;
+        const bool is_piv = in && rank == owner && r == lr;
+        if (is_piv && lane == 0) used[r] = 1;
+        act[u] = in && !is_piv && (used[rr[u]] == 0);
+        v[u] = rows[rr[u] * kPanelNB + lane];
       }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        Real ov = __shfl_xor_sync(0xffffffffu, b, o);
-        int orw = __shfl_xor_sync(0xffffffffu, br, o);
-        if (ov > b || (ov == b && orw < br)) {
-          b = ov;
-          br = orw;
-        }
+      for (int u = 0; u < kPanelUnroll; ++u) {
+        const C l = cmul(shfl_c(v[u], t), inv);
+        const C upd = csub(v[u], cmul(l, pc));
+        C r = v[u];
+        r.x = after_t ? upd.x : r.x;
+        r.y = after_t ? upd.y : r.y;
+        r.x = at_t ? l.x : r.x;
+        r.y = at_t ? l.y : r.y;
+        v[u] = r;
+        const Real a = (act[u] && next_t) ? pmag(r) : (Real)-1;
+        const bool take = a > best || (a == best && a >= 0 && rr[u] < brow);
+        best = take ? a : best;
+        brow = take ? rr[u] : brow;
       }
-      if (lane == 0) {
-        if (!(b > 0) || br >= m) {  // exactly singular column (or NaN): keep the diagonal
-          br = t;
-          if (!sh.singular) sh.singular = col0 + t + 1;
-        }
-        sh.piv_row = br;
-      }
+#pragma unroll
+      for (int u = 0; u < kPanelUnroll; ++u)
+        if (act[u]) rows[rr[u] * kPanelNB + lane] = v[u];
     }
-    __syncthreads();
-    const int p = sh.piv_row;
-    const int own_p = p / R, own_t = t / R;
-    // read the pivot row (all CTAs) and the target row (pivot owner)
-    if (tid < kPanelNB) {
-      const C* src = cluster.map_shared_rank(rows, own_p) + (long long)(p - own_p * R) * kPanelNB;
-      sh.prow[tid] = src[tid];
-      if (rank == own_p) {
-        const C* tsrc = cluster.map_shared_rank(rows, own_t) + (long long)(t - own_t * R) * kPanelNB;
-        sh.trow[tid] = tsrc[tid];
-      }
+    if (t + 1 < w) {
+      best = __shfl_sync(0xffffffffu, best, t + 1);
+      brow = __shfl_sync(0xffffffffu, brow, t + 1);
     }
-    cluster.sync();  // every remote read of this step is done before rows change
-    if (tid < kPanelNB) {
-      if (rank == own_t) rows[(t - own_t * R) * kPanelNB + tid] = sh.prow[tid];
-      if (rank == own_p && p != t) rows[(p - own_p * R) * kPanelNB + tid] = sh.trow[tid];
-    }
-    if (rank == 0 && tid == 0) ipiv[col0 + t] = col0 + p;
-    __syncthreads();
-    // ---- multipliers and rank-1 update of the remaining panel columns
-    const C piv = sh.prow[t];
-    const bool ok = (cabs1(piv) > 0);
-    for (int r = tid; r < rcount; r += kPanelThreads) {
-      if (r0 + r > t) {
-        C l = ok ? cdiv(rows[r * kPanelNB + t], piv) : czero<C>();
-        rows[r * kPanelNB + t] = l;
-      }
-    }
-    __syncthreads();
-    const int ncol = w - t - 1;
-    if (ncol > 0) {
-      for (int idx = tid; idx < rcount * ncol; idx += kPanelThreads) {
-        int r = idx / ncol, c = t + 1 + idx % ncol;
-        if (r0 + r > t) {
-          C l = rows[r * kPanelNB + t];
-          rows[r * kPanelNB + c] = csub(rows[r * kPanelNB + c], cmul(l, sh.prow[c]));
-        }
-      }
-    }
-    __syncthreads();
   }
+  // no CTA may leave while others can still read its published slots
+  if (cs > 1) cluster.sync(); else __syncthreads();
   for (int idx = tid; idx < rcount * kPanelNB; idx += kPanelThreads) {
-    int r = idx / kPanelNB, c = idx % kPanelNB;
-    if (c < w) A[(long long)(col0 + r0 + r) * ld + col0 + c] = rows[idx];
+    int r = idx >> 5, c = idx & 31;
+    if (c < w) A[(long long)phys[r] * ld + col + c] = rows[idx];
   }
-  if (rank == 0 && tid == 0 && sh.singular && info) atomicCAS(info, 0, sh.singular);
-  cluster.sync();  // no CTA leaves while others may still read its shared memory
+  if (rank == 0 && wid == 0) {
+    replay_pivots(w, sh.perm, ipiv, ipiv_base, rowmap);
+    if (lane == 0 && sh.singular && info) atomicCAS(info, 0, ipiv_base + sh.singular);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Register-resident panel: warp w of CTA `rank` holds panel rows
+// r = w + 8 j (j < kRegRows) of the CTA's R rows, lane c holding column c, so a
+// column step is shuffles and FMAs only.  Candidate exchange as above: each
+// warp publishes its best row, warp 0 reduces, one cluster barrier, warp 0
+// gathers the cs candidates and the winning row.
+constexpr int kRegWarps = 8;
+constexpr int kRegThreads = 32 * kRegWarps;
+// rows per warp: 48 for complex64, 32 for complex128 (register budget)
+template <typename C> struct RegRows { static constexpr int value = 48; };
+template <> struct RegRows<double2> { static constexpr int value = 32; };
+constexpr int kRegRowsMax = 48;
+
+template <typename C>
+struct RegPanelShared {
+  R_t<C> wval[kRegWarps];
+  int wrow[kRegWarps];
+  C wrowdata[2][kRegWarps][kPanelNB];  // each warp's best row (double buffered)
+  R_t<C> cval[2];
+  int crow[2];
+  int cwarp[2];
+  int p;
+  C prow[kPanelNB];
+  int perm[kPanelNB];
+  int singular;
+  int mk[2 * kPanelNB];
+  int mv[2 * kPanelNB];
+  int mo[2 * kPanelNB];
+  int32_t phys[kRegWarps * kRegRowsMax];  // storage rows of this CTA's panel rows
+};
+
+template <typename C>
+__global__ void __launch_bounds__(kRegThreads, 1) panel_lu_reg_kernel(int m, int w, C* __restrict__ A, long long ld,
+                                                                      int col, int32_t* __restrict__ rowmap,
+                                                                      int32_t* __restrict__ ipiv, int ipiv_base,
+                                                                      int* __restrict__ info, int R) {
+  using Real = R_t<C>;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int cs = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  __shared__ RegPanelShared<C> sh;
+  const int r0 = rank * R;
+  const int rcount = max(0, min(R, m - r0));
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nmine = rcount > wid ? (rcount - wid + kRegWarps - 1) / kRegWarps : 0;  // rows of this warp
+
+  constexpr int kRegRows = RegRows<C>::value;
+  for (int r = tid; r < rcount; r += kRegThreads) sh.phys[r] = rowmap[r0 + r];
+  if (tid == 0) sh.singular = 0;
+  __syncthreads();
+  C v[kRegRows];
+  uint64_t active = 0;
+#pragma unroll
+  for (int j = 0; j < kRegRows; ++j) {
+    v[j] = czero<C>();
+    if (j < nmine) {
+      const int r = wid + kRegWarps * j;
+      if (lane < w) v[j] = A[(long long)sh.phys[r] * ld + col + lane];
+      active |= 1ull << j;
+    }
+  }
+
+  // straight-line code (selects, no branches) so the unrolled rows interleave
+  auto warp_cand = [&](int c, Real& b, int& bj) {
+    b = -1;
+    bj = INT_MAX;
+#pragma unroll
+    for (int j = 0; j < kRegRows; ++j) {
+      const Real a = ((active >> j) & 1ull) ? pmag(v[j]) : (Real)-1;
+      const bool take = a > b;  // rows are visited in increasing j: first max wins
+      b = take ? a : b;
+      bj = take ? j : bj;
+    }
+    b = __shfl_sync(0xffffffffu, b, c);
+    bj = __shfl_sync(0xffffffffu, bj, c);
+  };
+  Real best;
+  int bj;
+  warp_cand(0, best, bj);
+
+  for (int t = 0; t < w; ++t) {
+    const int buf = t & 1;
+    // publish this warp's candidate (value, local row, row data)
+    C sel = czero<C>();
+#pragma unroll
+    for (int j = 0; j < kRegRows; ++j) {
+      sel.x = (j == bj) ? v[j].x : sel.x;
+      sel.y = (j == bj) ? v[j].y : sel.y;
+    }
+    sh.wrowdata[buf][wid][lane] = sel;
+    if (lane == 0) {
+      sh.wval[wid] = best;
+      sh.wrow[wid] = bj < nmine ? wid + kRegWarps * bj : INT_MAX;
+    }
+    __syncthreads();
+    if (wid == 0) {
+      Real b = lane < kRegWarps ? sh.wval[lane] : (Real)-1;
+      int br = lane < kRegWarps ? sh.wrow[lane] : INT_MAX;
+      warp_argmax<C>(b, br);
+      if (lane == 0) {
+        sh.cval[buf] = br < rcount ? b : (Real)-1;
+        sh.crow[buf] = br < rcount ? r0 + br : INT_MAX;
+        sh.cwarp[buf] = br < rcount ? br % kRegWarps : 0;
+      }
+    }
+    if (cs > 1) cluster.sync(); else __syncthreads();
+    if (wid == 0) {
+      Real b = -1;
+      int br = INT_MAX;
+      if (lane < cs) {
+        const RegPanelShared<C>* rs = (cs > 1) ? cluster.map_shared_rank(&sh, lane) : &sh;
+        b = rs->cval[buf];
+        br = rs->crow[buf];
+      }
+      warp_argmax<C>(b, br);
+      const int p = min(br, m - 1);  // an unused row always exists: br < m
+      const int owner = p / R;
+      const RegPanelShared<C>* os = (cs > 1) ? cluster.map_shared_rank(&sh, owner) : &sh;
+      sh.prow[lane] = os->wrowdata[buf][os->cwarp[buf]][lane];
+      if (lane == 0) {
+        sh.p = p;
+        sh.perm[t] = p;
+        if (!(b > 0) && !sh.singular) sh.singular = t + 1;
+      }
+    }
+    __syncthreads();
+    const int p = sh.p;
+    const int owner = p / R, lr = p - owner * R;
+    if (rank == owner && (lr % kRegWarps) == wid) active &= ~(1ull << (lr / kRegWarps));
+    const C pc = sh.prow[lane];
+    const C piv = shfl_c(pc, t);
+    const bool ok = cabs1(piv) > 0;
+    const C inv = ok ? cdiv(cmake<C>(1.0, 0.0), piv) : czero<C>();
+    const bool at_t = lane == t, after_t = lane > t;
+#pragma unroll
+    for (int j = 0; j < kRegRows; ++j) {
+      const C l = cmul(shfl_c(v[j], t), inv);
+      const C u = csub(v[j], cmul(l, pc));
+      const bool act = (active >> j) & 1ull;
+      C r = v[j];
+      r.x = after_t ? u.x : r.x;
+      r.y = after_t ? u.y : r.y;
+      r.x = at_t ? l.x : r.x;
+      r.y = at_t ? l.y : r.y;
+      v[j].x = act ? r.x : v[j].x;
+      v[j].y = act ? r.y : v[j].y;
+    }
+    if (t + 1 < w) warp_cand(t + 1, best, bj);
+  }
+  if (cs > 1) cluster.sync(); else __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kRegRows; ++j)
+    if (j < nmine && lane < w) A[(long long)sh.phys[wid + kRegWarps * j] * ld + col + lane] = v[j];
+  if (rank == 0 && wid == 0) {
+    replay_pivots(w, sh.perm, ipiv, ipiv_base, rowmap);
+    if (lane == 0 && sh.singular && info) atomicCAS(info, 0, ipiv_base + sh.singular);
+  }
 }
 
 template <typename C>
-static int panel_lu(const LaContext& ctx, int n, C* A, long long ld, int32_t* ipiv, int col0, int w) {
-  const int m = n - col0;
-  const size_t row_bytes = sizeof(C) * kPanelNB;
+static int panel_lu(const LaContext& ctx, int m, int w, C* A, long long ld, int col, int32_t* rowmap, int32_t* ipiv,
+                    int ipiv_base) {
+  constexpr int kRegCap = kRegWarps * RegRows<C>::value;  // rows per CTA
+  if (m <= 16 * kRegCap) {
+    int cs = ceil_div(m, kRegCap);
+    int R = ceil_div(m, cs);
+    auto kern = panel_lu_reg_kernel<C>;
+    BEM_CUDA_CHECK(set_kernel_attrs_once(kern, 0, true));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs, 1, 1);
+    cfg.blockDim = dim3(kRegThreads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ctx.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BEM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, m, w, A, ld, col, rowmap, ipiv, ipiv_base, ctx.dinfo, R));
+    count_launch();
+    return BEM200_OK;
+  }
+  const size_t row_bytes = sizeof(C) * kPanelNB + sizeof(int32_t) + 1;
   const size_t max_smem = 200 * 1024;
   int cs = 1;
   while ((size_t)ceil_div(m, cs) * row_bytes > max_smem && cs < 16) cs *= 2;
   int R = ceil_div(m, cs);
-  size_t smem = (size_t)R * row_bytes;
+  size_t smem = (size_t)R * row_bytes + 16;
   BEM_REQUIRE(smem <= max_smem, BEM200_ERR_UNSUPPORTED,
               "panel_lu: panel of %d rows does not fit a 16-CTA cluster", m);
   auto kern = panel_lu_kernel<C>;
-  BEM_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  if (cs > 8) BEM_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  BEM_CUDA_CHECK(set_kernel_attrs_once(kern, (int)(max_smem + 1024), true));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs, 1, 1);
   cfg.blockDim = dim3(kPanelThreads, 1, 1);
@@ -346,7 +573,8 @@ static int panel_lu(const LaContext& ctx, int n, C* A, long long ld, int32_t* ip
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  BEM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, n, col0, w, A, ld, ipiv, ctx.dinfo, R));
+  BEM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, m, w, A, ld, col, rowmap, ipiv, ipiv_base, ctx.dinfo, R));
+  count_launch();
   return BEM200_OK;
 }
 
@@ -359,19 +587,18 @@ constexpr int kTrsmThreads = 128;
 
 // B[0:m, c] <- T^-1 B[0:m, c]; lower = unit lower (L), else upper non-unit (U)
 template <typename C, bool kLower>
-__global__ void __launch_bounds__(kTrsmThreads) trsm_left_leaf(int m, int ncols, const C* __restrict__ T, long long ldt,
-                                                               C* __restrict__ B, long long ldb) {
+__global__ void __launch_bounds__(kTrsmThreads) trsm_left_leaf(int m, int ncols, RowView<C> T, RowView<C> B) {
   extern __shared__ __align__(16) unsigned char trsm_smem[];
   auto Ts = reinterpret_cast<C(*)[kTrsmNB + 1]>(trsm_smem);
   auto Bs = reinterpret_cast<C(*)[kTrsmThreads]>(trsm_smem + sizeof(C) * kTrsmNB * (kTrsmNB + 1));
   const int c0 = blockIdx.x * kTrsmThreads;
   for (int idx = threadIdx.x; idx < m * m; idx += kTrsmThreads) {
     int r = idx / m, c = idx % m;
-    Ts[r][c] = T[(long long)r * ldt + c];
+    Ts[r][c] = T.at(r, c);
   }
   for (int idx = threadIdx.x; idx < m * kTrsmThreads; idx += kTrsmThreads) {
     int r = idx / kTrsmThreads, c = idx % kTrsmThreads;
-    Bs[r][c] = (c0 + c < ncols) ? B[(long long)r * ldb + c0 + c] : czero<C>();
+    Bs[r][c] = (c0 + c < ncols) ? B.at(r, c0 + c) : czero<C>();
   }
   __syncthreads();
   const int c = threadIdx.x;
@@ -391,37 +618,34 @@ __global__ void __launch_bounds__(kTrsmThreads) trsm_left_leaf(int m, int ncols,
   __syncthreads();
   for (int idx = threadIdx.x; idx < m * kTrsmThreads; idx += kTrsmThreads) {
     int r = idx / kTrsmThreads, cc = idx % kTrsmThreads;
-    if (c0 + cc < ncols) B[(long long)r * ldb + c0 + cc] = Bs[r][cc];
+    if (c0 + cc < ncols) B.at(r, c0 + cc) = Bs[r][cc];
   }
 }
 
 // X[r, 0:m] <- X[r, 0:m] T^-1 ; upper = non-unit upper (U), else unit lower (L)
 template <typename C, bool kUpper>
-__global__ void __launch_bounds__(kTrsmThreads) trsm_right_leaf(int m, int nrows, const C* __restrict__ T,
-                                                                long long ldt, C* __restrict__ X, long long ldx) {
+__global__ void __launch_bounds__(kTrsmThreads) trsm_right_leaf(int m, int nrows, RowView<C> T, RowView<C> X) {
   extern __shared__ __align__(16) unsigned char trsm_smem[];
   auto Ts = reinterpret_cast<C(*)[kTrsmNB + 1]>(trsm_smem);
   auto Xs = reinterpret_cast<C(*)[kTrsmNB + 1]>(trsm_smem + sizeof(C) * kTrsmNB * (kTrsmNB + 1));
   const int r0 = blockIdx.x * kTrsmThreads;
   for (int idx = threadIdx.x; idx < m * m; idx += kTrsmThreads) {
     int r = idx / m, c = idx % m;
-    Ts[r][c] = T[(long long)r * ldt + c];
+    Ts[r][c] = T.at(r, c);
   }
   for (int idx = threadIdx.x; idx < m * kTrsmThreads; idx += kTrsmThreads) {
     int r = idx / m, c = idx % m;
-    Xs[r][c] = (r0 + r < nrows) ? X[(long long)(r0 + r) * ldx + c] : czero<C>();
+    Xs[r][c] = (r0 + r < nrows) ? X.at(r0 + r, c) : czero<C>();
   }
   __syncthreads();
   const int r = threadIdx.x;
   if (kUpper) {
-    // x U = y: x_c = (y_c - sum_{q<c} x_q U_qc) / U_cc
     for (int c = 0; c < m; ++c) {
       C s = Xs[r][c];
       for (int q = 0; q < c; ++q) s = csub(s, cmul(Xs[r][q], Ts[q][c]));
       Xs[r][c] = cdiv(s, Ts[c][c]);
     }
   } else {
-    // x L = y, L unit lower: x_c = y_c - sum_{q>c} x_q L_qc
     for (int c = m - 1; c >= 0; --c) {
       C s = Xs[r][c];
       for (int q = c + 1; q < m; ++q) s = csub(s, cmul(Xs[r][q], Ts[q][c]));
@@ -431,7 +655,7 @@ __global__ void __launch_bounds__(kTrsmThreads) trsm_right_leaf(int m, int nrows
   __syncthreads();
   for (int idx = threadIdx.x; idx < m * kTrsmThreads; idx += kTrsmThreads) {
     int rr = idx / m, c = idx % m;
-    if (r0 + rr < nrows) X[(long long)(r0 + rr) * ldx + c] = Xs[rr][c];
+    if (r0 + rr < nrows) X.at(r0 + rr, c) = Xs[rr][c];
   }
 }
 
@@ -442,7 +666,7 @@ static size_t trsm_smem_bytes() {
 
 template <typename K>
 static int prep_smem(K kern, size_t bytes) {
-  BEM_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  BEM_CUDA_CHECK(set_kernel_attrs_once(kern, (int)bytes, false));
   return BEM200_OK;
 }
 
@@ -457,173 +681,349 @@ static int split_point(int m) {
 
 // B <- L^-1 B, L unit lower m x m (strict lower part of T)
 template <typename C>
-static int trsm_llu(const LaContext& ctx, int m, int ncols, const C* T, long long ldt, C* B, long long ldb) {
+static int trsm_llu(const LaContext& ctx, int m, int ncols, RowView<C> T, RowView<C> B) {
   if (m <= 0 || ncols <= 0) return BEM200_OK;
   if (m <= kTrsmNB) {
-    { int _st = prep_smem(trsm_left_leaf<C, true>, trsm_smem_bytes<C>()); if (_st) return _st; }
-    trsm_left_leaf<C, true><<<ceil_div(ncols, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(m, ncols, T, ldt, B, ldb);
+    int st = prep_smem(trsm_left_leaf<C, true>, trsm_smem_bytes<C>());
+    if (st) return st;
+    trsm_left_leaf<C, true><<<ceil_div(ncols, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(
+        m, ncols, T, B);
     BEM_LAUNCH_CHECK();
     return BEM200_OK;
   }
   int m1 = split_point(m);
-  int st = trsm_llu(ctx, m1, ncols, T, ldt, B, ldb);
+  int st = trsm_llu(ctx, m1, ncols, T, B);
   if (st) return st;
-  st = gemm<C>(ctx, m - m1, ncols, m1, neg_one<C>(), T + (long long)m1 * ldt, ldt, B, ldb, one<C>(),
-               B + (long long)m1 * ldb, ldb);
+  st = gemm_v<C>(ctx, m - m1, ncols, m1, neg_one<C>(), T.sub(m1, 0), B, one<C>(), B.sub(m1, 0));
   if (st) return st;
-  return trsm_llu(ctx, m - m1, ncols, T + (long long)m1 * ldt + m1, ldt, B + (long long)m1 * ldb, ldb);
+  return trsm_llu(ctx, m - m1, ncols, T.sub(m1, m1), B.sub(m1, 0));
 }
 
 // B <- U^-1 B, U upper non-unit
 template <typename C>
-static int trsm_lun(const LaContext& ctx, int m, int ncols, const C* T, long long ldt, C* B, long long ldb) {
+static int trsm_lun(const LaContext& ctx, int m, int ncols, RowView<C> T, RowView<C> B) {
   if (m <= 0 || ncols <= 0) return BEM200_OK;
   if (m <= kTrsmNB) {
-    { int _st = prep_smem(trsm_left_leaf<C, false>, trsm_smem_bytes<C>()); if (_st) return _st; }
-    trsm_left_leaf<C, false><<<ceil_div(ncols, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(m, ncols, T, ldt, B,
-                                                                                              ldb);
+    int st = prep_smem(trsm_left_leaf<C, false>, trsm_smem_bytes<C>());
+    if (st) return st;
+    trsm_left_leaf<C, false><<<ceil_div(ncols, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(
+        m, ncols, T, B);
     BEM_LAUNCH_CHECK();
     return BEM200_OK;
   }
   int m1 = split_point(m);
-  int st = trsm_lun(ctx, m - m1, ncols, T + (long long)m1 * ldt + m1, ldt, B + (long long)m1 * ldb, ldb);
+  int st = trsm_lun(ctx, m - m1, ncols, T.sub(m1, m1), B.sub(m1, 0));
   if (st) return st;
-  st = gemm<C>(ctx, m1, ncols, m - m1, neg_one<C>(), T + m1, ldt, B + (long long)m1 * ldb, ldb, one<C>(), B, ldb);
+  st = gemm_v<C>(ctx, m1, ncols, m - m1, neg_one<C>(), T.sub(0, m1), B.sub(m1, 0), one<C>(), B);
   if (st) return st;
-  return trsm_lun(ctx, m1, ncols, T, ldt, B, ldb);
+  return trsm_lun(ctx, m1, ncols, T, B);
 }
 
 // X <- X U^-1, X nrows x m
 template <typename C>
-static int trsm_run(const LaContext& ctx, int m, int nrows, const C* T, long long ldt, C* X, long long ldx) {
+static int trsm_run(const LaContext& ctx, int m, int nrows, RowView<C> T, RowView<C> X) {
   if (m <= 0 || nrows <= 0) return BEM200_OK;
   if (m <= kTrsmNB) {
-    { int _st = prep_smem(trsm_right_leaf<C, true>, trsm_smem_bytes<C>()); if (_st) return _st; }
-    trsm_right_leaf<C, true><<<ceil_div(nrows, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(m, nrows, T, ldt, X,
-                                                                                             ldx);
+    int st = prep_smem(trsm_right_leaf<C, true>, trsm_smem_bytes<C>());
+    if (st) return st;
+    trsm_right_leaf<C, true><<<ceil_div(nrows, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(
+        m, nrows, T, X);
     BEM_LAUNCH_CHECK();
     return BEM200_OK;
   }
   int m1 = split_point(m);
-  int st = trsm_run(ctx, m1, nrows, T, ldt, X, ldx);
+  int st = trsm_run(ctx, m1, nrows, T, X);
   if (st) return st;
-  // X2 -= X1 U12
-  st = gemm<C>(ctx, nrows, m - m1, m1, neg_one<C>(), X, ldx, T + m1, ldt, one<C>(), X + m1, ldx);
+  st = gemm_v<C>(ctx, nrows, m - m1, m1, neg_one<C>(), X, T.sub(0, m1), one<C>(), X.sub(0, m1));
   if (st) return st;
-  return trsm_run(ctx, m - m1, nrows, T + (long long)m1 * ldt + m1, ldt, X + m1, ldx);
+  return trsm_run(ctx, m - m1, nrows, T.sub(m1, m1), X.sub(0, m1));
 }
 
 // X <- X L^-1, L unit lower
 template <typename C>
-static int trsm_rlu(const LaContext& ctx, int m, int nrows, const C* T, long long ldt, C* X, long long ldx) {
+static int trsm_rlu(const LaContext& ctx, int m, int nrows, RowView<C> T, RowView<C> X) {
   if (m <= 0 || nrows <= 0) return BEM200_OK;
   if (m <= kTrsmNB) {
-    { int _st = prep_smem(trsm_right_leaf<C, false>, trsm_smem_bytes<C>()); if (_st) return _st; }
-    trsm_right_leaf<C, false><<<ceil_div(nrows, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(m, nrows, T, ldt, X,
-                                                                                              ldx);
+    int st = prep_smem(trsm_right_leaf<C, false>, trsm_smem_bytes<C>());
+    if (st) return st;
+    trsm_right_leaf<C, false><<<ceil_div(nrows, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(
+        m, nrows, T, X);
     BEM_LAUNCH_CHECK();
     return BEM200_OK;
   }
   int m1 = split_point(m);
-  int st = trsm_rlu(ctx, m - m1, nrows, T + (long long)m1 * ldt + m1, ldt, X + m1, ldx);
+  int st = trsm_rlu(ctx, m - m1, nrows, T.sub(m1, m1), X.sub(0, m1));
   if (st) return st;
-  // X1 -= X2 L21
-  st = gemm<C>(ctx, nrows, m1, m - m1, neg_one<C>(), X + m1, ldx, T + (long long)m1 * ldt, ldt, one<C>(), X, ldx);
+  st = gemm_v<C>(ctx, nrows, m1, m - m1, neg_one<C>(), X.sub(0, m1), T.sub(m1, 0), one<C>(), X);
   if (st) return st;
-  return trsm_rlu(ctx, m1, nrows, T, ldt, X, ldx);
+  return trsm_rlu(ctx, m1, nrows, T, X);
 }
 
-// ===================================================================== LU
+// ===================================================================== blocked TRSV
+// Solves T x = b in place for nrhs <= 16 right-hand sides (X is n x nrhs, ld
+// nrhs).  Row block I (64 rows) is processed by the CTA that drew ticket I from
+// an atomic counter; it consumes the solution blocks it depends on as their
+// flags are set, then solves its diagonal block and publishes its flag.  A CTA
+// only waits on blocks whose tickets were drawn earlier, so every wait ends;
+// each wait is nonetheless bounded and reports BEM200_ERR_TIMEOUT in *status.
+constexpr int kTrsvBS = 64;
+constexpr int kTrsvMaxRhs = 16;
+constexpr long long kSpinLimit = 1LL << 22;
+
+template <typename C, bool kLower>
+__global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowView<C> T, C* __restrict__ X,
+                                                          int* __restrict__ flags, int* __restrict__ ticket,
+                                                          int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char trsv_smem[];
+  auto tile = reinterpret_cast<C(*)[kTrsvBS + 1]>(trsv_smem);                                  // 64 x 65
+  auto xs = reinterpret_cast<C(*)[kTrsvMaxRhs]>(trsv_smem + sizeof(C) * kTrsvBS * (kTrsvBS + 1));  // 64 x 16
+  auto xj = xs + kTrsvBS;                                                                      // 64 x 16
+  __shared__ int sI, sabort;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nblk = ceil_div(n, kTrsvBS);
+  if (tid == 0) {
+    sI = atomicAdd(ticket, 1);
+    sabort = 0;
+  }
+  __syncthreads();
+  const int tk = sI;
+  if (tk >= nblk) return;
+  const int I = kLower ? tk : nblk - 1 - tk;
+  const int r0 = I * kTrsvBS, rb = min(kTrsvBS, n - r0);
+  for (int idx = tid; idx < kTrsvBS * nrhs; idx += 256) {
+    int r = idx / nrhs, q = idx % nrhs;
+    xs[r][q] = (r < rb) ? X[(long long)(r0 + r) * nrhs + q] : czero<C>();
+  }
+  const int nsrc = kLower ? I : nblk - 1 - I;
+  for (int s = 0; s < nsrc; ++s) {
+    const int J = kLower ? s : nblk - 1 - s;
+    const int c0 = J * kTrsvBS, cb = min(kTrsvBS, n - c0);
+    if (tid == 0) {
+      long long spins = 0;
+      while (atomicAdd(&flags[J], 0) == 0) {
+        if (++spins > kSpinLimit) {
+          atomicExch(status, BEM200_ERR_TIMEOUT);
+          sabort = 1;
+          break;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    if (sabort) break;
+    for (int idx = tid; idx < kTrsvBS * nrhs; idx += 256) {
+      int c = idx / nrhs, q = idx % nrhs;
+      xj[c][q] = (c < cb) ? __ldcg(reinterpret_cast<const C*>(X) + (long long)(c0 + c) * nrhs + q) : czero<C>();
+    }
+    for (int idx = tid; idx < rb * kTrsvBS; idx += 256) {
+      int r = idx >> 6, c = idx & 63;
+      tile[r][c] = (c < cb) ? T.at(r0 + r, c0 + c) : czero<C>();
+    }
+    __syncthreads();
+    for (int idx = tid; idx < rb * nrhs; idx += 256) {
+      int r = idx / nrhs, q = idx % nrhs;
+      C acc = xs[r][q];
+      for (int c = 0; c < cb; ++c) acc = csub(acc, cmul(tile[r][c], xj[c][q]));
+      xs[r][q] = acc;
+    }
+    __syncthreads();
+  }
+  // diagonal block
+  for (int idx = tid; idx < rb * kTrsvBS; idx += 256) {
+    int r = idx >> 6, c = idx & 63;
+    tile[r][c] = (c < rb) ? T.at(r0 + r, r0 + c) : czero<C>();
+  }
+  __syncthreads();
+  // warp q solves right-hand side q; lanes split the dot products
+  for (int q = wid; q < nrhs; q += 8) {
+    if (kLower) {
+      for (int r = 0; r < rb; ++r) {
+        C part = czero<C>();
+        for (int c = lane; c < r; c += 32) part = cadd(part, cmul(tile[r][c], xs[c][q]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          part.x += __shfl_xor_sync(0xffffffffu, part.x, o);
+          part.y += __shfl_xor_sync(0xffffffffu, part.y, o);
+        }
+        if (lane == 0) xs[r][q] = csub(xs[r][q], part);
+        __syncwarp();
+      }
+    } else {
+      for (int r = rb - 1; r >= 0; --r) {
+        C part = czero<C>();
+        for (int c = r + 1 + lane; c < rb; c += 32) part = cadd(part, cmul(tile[r][c], xs[c][q]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          part.x += __shfl_xor_sync(0xffffffffu, part.x, o);
+          part.y += __shfl_xor_sync(0xffffffffu, part.y, o);
+        }
+        if (lane == 0) xs[r][q] = cdiv(csub(xs[r][q], part), tile[r][r]);
+        __syncwarp();
+      }
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < rb * nrhs; idx += 256) {
+    int r = idx / nrhs, q = idx % nrhs;
+    X[(long long)(r0 + r) * nrhs + q] = xs[r][q];
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) atomicExch(&flags[I], 1);
+}
+
 template <typename C>
-static int getrf_rec(const LaContext& ctx, int n, C* A, long long ld, int32_t* ipiv, int col0, int w) {
-  if (w <= kPanelNB) return panel_lu<C>(ctx, n, A, ld, ipiv, col0, w);
+static size_t trsv_smem_bytes() {
+  return sizeof(C) * (kTrsvBS * (kTrsvBS + 1) + 2 * kTrsvBS * kTrsvMaxRhs);
+}
+
+template <typename C, bool kLower>
+static int trsv_blocked(const LaContext& ctx, int n, int nrhs, RowView<C> T, C* X, int* iscratch) {
+  const int nblk = ceil_div(n, kTrsvBS);
+  // iscratch: flags [0, nblk), ticket [nblk], local status [nblk + 1]
+  BEM_CUDA_CHECK(cudaMemsetAsync(iscratch, 0, sizeof(int) * (nblk + 2), ctx.stream));
+  auto kern = trsv_blocked_kernel<C, kLower>;
+  int st = prep_smem(kern, trsv_smem_bytes<C>());
+  if (st) return st;
+  kern<<<nblk, 256, trsv_smem_bytes<C>(), ctx.stream>>>(n, nrhs, T, X, iscratch, iscratch + nblk,
+                                                        ctx.dstatus ? ctx.dstatus : iscratch + nblk + 1);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+// ===================================================================== LU driver
+__global__ void iota_kernel(int n, int32_t* __restrict__ a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+
+template <typename C>
+static int getrf_rec(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv, int col0,
+                     int w) {
+  if (w <= kPanelNB) return panel_lu<C>(ctx, n - col0, w, A, ld, col0, rowmap + col0, ipiv + col0, col0);
   int w1 = split_point(w);
-  int st = getrf_rec(ctx, n, A, ld, ipiv, col0, w1);
+  int st = getrf_rec(ctx, n, A, ld, rowmap, ipiv, col0, w1);
   if (st) return st;
-  // right half of this column range: apply the left half's swaps
-  st = laswp(ctx, A, ld, col0 + w1, col0 + w, ipiv, col0, col0 + w1);
-  if (st) return st;
-  C* A11 = A + (long long)col0 * ld + col0;
+  RowView<C> V{A, ld, rowmap + col0, col0};  // logical rows from col0, columns from col0
   // U12 = L11^-1 A12
-  st = trsm_llu(ctx, w1, w - w1, A11, ld, A11 + w1, ld);
+  st = trsm_llu<C>(ctx, w1, w - w1, V, V.sub(0, w1));
   if (st) return st;
   // A22 -= L21 U12
-  st = gemm<C>(ctx, n - col0 - w1, w - w1, w1, neg_one<C>(), A11 + (long long)w1 * ld, ld, A11 + w1, ld, one<C>(),
-               A11 + (long long)w1 * ld + w1, ld);
+  st = gemm_v<C>(ctx, n - col0 - w1, w - w1, w1, neg_one<C>(), V.sub(w1, 0), V.sub(0, w1), one<C>(), V.sub(w1, w1));
   if (st) return st;
-  st = getrf_rec(ctx, n, A, ld, ipiv, col0 + w1, w - w1);
-  if (st) return st;
-  // left half: apply the right half's swaps
-  return laswp(ctx, A, ld, col0, col0 + w1, ipiv, col0 + w1, col0 + w);
+  return getrf_rec(ctx, n, A, ld, rowmap, ipiv, col0 + w1, w - w1);
 }
 
 template <typename C>
-int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* ipiv) {
-  BEM_REQUIRE(n > 0 && A && ipiv && ld >= n, BEM200_ERR_ARG, "getrf: bad arguments");
-  return getrf_rec(ctx, n, A, ld, ipiv, 0, n);
+int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv, int32_t* scratch) {
+  (void)scratch;
+  BEM_REQUIRE(n > 0 && A && rowmap && ipiv && ld >= n, BEM200_ERR_ARG, "getrf: bad arguments");
+  iota_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(n, rowmap);
+  BEM_LAUNCH_CHECK();
+  return getrf_rec(ctx, n, A, ld, rowmap, ipiv, 0, n);
+}
+
+// ===================================================================== solves
+// out[i, :] = in[map[i], :]
+template <typename C>
+__global__ void gather_rows_kernel(int n, int ncols, const C* __restrict__ in, long long ldi,
+                                   const int32_t* __restrict__ map, C* __restrict__ out, long long ldo) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * ncols) return;
+  int i = (int)(idx / ncols), c = (int)(idx % ncols);
+  out[(long long)i * ldo + c] = in[(long long)map[i] * ldi + c];
+}
+
+// Y[r, map[i]] = X[r, i]
+template <typename C>
+__global__ void scatter_cols_kernel(int m, int n, const C* __restrict__ X, long long ldx,
+                                    const int32_t* __restrict__ map, C* __restrict__ Y, long long ldy) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)m * n) return;
+  int r = (int)(idx / n), i = (int)(idx % n);
+  Y[(long long)r * ldy + map[i]] = X[(long long)r * ldx + i];
+}
+
+static size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+
+template <typename C>
+size_t solve_left_scratch_bytes(int n, int nrhs) {
+  return round256(sizeof(C) * (size_t)n * nrhs) + round256(sizeof(int) * (ceil_div(n, kTrsvBS) + 2));
 }
 
 template <typename C>
-int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld, const int32_t* ipiv, C* B,
-               long long ldb) {
+int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld, const int32_t* rowmap, C* B,
+               long long ldb, void* scratch) {
   if (nrhs <= 0) return BEM200_OK;
-  int st = laswp(ctx, B, ldb, 0, nrhs, ipiv, 0, n);
-  if (st) return st;
-  st = trsm_llu(ctx, n, nrhs, LU, ld, B, ldb);
-  if (st) return st;
-  return trsm_lun(ctx, n, nrhs, LU, ld, B, ldb);
+  BEM_REQUIRE(scratch, BEM200_ERR_ARG, "solve_left: scratch required");
+  C* Y = reinterpret_cast<C*>(scratch);
+  int* iscr = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) + round256(sizeof(C) * (size_t)n * nrhs));
+  long long tot = (long long)n * nrhs;
+  gather_rows_kernel<C><<<ceil_div(tot, 256), 256, 0, ctx.stream>>>(n, nrhs, B, ldb, rowmap, Y, nrhs);
+  BEM_LAUNCH_CHECK();
+  RowView<C> T{const_cast<C*>(LU), ld, rowmap, 0};
+  int st;
+  if (nrhs <= kTrsvMaxRhs) {
+    if ((st = trsv_blocked<C, true>(ctx, n, nrhs, T, Y, iscr))) return st;
+    if ((st = trsv_blocked<C, false>(ctx, n, nrhs, T, Y, iscr))) return st;
+  } else {
+    if ((st = trsm_llu<C>(ctx, n, nrhs, T, plain(Y, nrhs)))) return st;
+    if ((st = trsm_lun<C>(ctx, n, nrhs, T, plain(Y, nrhs)))) return st;
+  }
+  BEM_CUDA_CHECK(cudaMemcpy2DAsync(B, ldb * sizeof(C), Y, nrhs * sizeof(C), nrhs * sizeof(C), n,
+                                   cudaMemcpyDeviceToDevice, ctx.stream));
+  return BEM200_OK;
 }
 
 template <typename C>
-int solve_right(const LaContext& ctx, int n, int m, const C* LU, long long ld, const int32_t* ipiv, C* X,
+int solve_right(const LaContext& ctx, int n, int m, const C* LU, long long ld, const int32_t* rowmap, C* X,
                 long long ldx, C* tmp) {
   // X A = Y with P A = L U  =>  X = Y U^-1 L^-1 P
   if (m <= 0) return BEM200_OK;
-  int st = trsm_run(ctx, n, m, LU, ld, X, ldx);
+  RowView<C> T{const_cast<C*>(LU), ld, rowmap, 0};
+  int st = trsm_run<C>(ctx, n, m, T, plain(X, ldx));
   if (st) return st;
-  st = trsm_rlu(ctx, n, m, LU, ld, X, ldx);
+  st = trsm_rlu<C>(ctx, n, m, T, plain(X, ldx));
   if (st) return st;
-  int32_t* perm = reinterpret_cast<int32_t*>(tmp + (long long)m * n);
-  ipiv_to_perm_kernel<<<1, 1, 0, ctx.stream>>>(n, ipiv, perm);
-  BEM_LAUNCH_CHECK();
   long long tot = (long long)m * n;
-  colperm_kernel<C><<<ceil_div(tot, 256), 256, 0, ctx.stream>>>(m, n, X, ldx, perm, tmp, n);
+  scatter_cols_kernel<C><<<ceil_div(tot, 256), 256, 0, ctx.stream>>>(m, n, X, ldx, rowmap, tmp, n);
   BEM_LAUNCH_CHECK();
   BEM_CUDA_CHECK(cudaMemcpy2DAsync(X, ldx * sizeof(C), tmp, n * sizeof(C), n * sizeof(C), m,
                                    cudaMemcpyDeviceToDevice, ctx.stream));
   return BEM200_OK;
 }
 
+// B[i, j] = (j == map[i])  (the permutation matrix P of P A = L U)
 template <typename C>
-__global__ void set_identity_kernel(int n, C* A, long long ld) {
+__global__ void perm_matrix_kernel(int n, const int32_t* __restrict__ map, C* A, long long ld) {
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)n * n) return;
   int r = (int)(idx / n), c = (int)(idx % n);
-  A[(long long)r * ld + c] = (r == c) ? cmake<C>(1.0, 0.0) : czero<C>();
+  A[(long long)r * ld + c] = (c == map[r]) ? cmake<C>(1.0, 0.0) : czero<C>();
 }
 
 template <typename C>
-int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_t* ipiv, C* Inv, long long ldi) {
-  set_identity_kernel<C><<<ceil_div((long long)n * n, 256), 256, 0, ctx.stream>>>(n, Inv, ldi);
+int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_t* rowmap, C* Inv, long long ldi) {
+  perm_matrix_kernel<C><<<ceil_div((long long)n * n, 256), 256, 0, ctx.stream>>>(n, rowmap, Inv, ldi);
   BEM_LAUNCH_CHECK();
-  return solve_left(ctx, n, n, LU, ld, ipiv, Inv, ldi);
+  RowView<C> T{const_cast<C*>(LU), ld, rowmap, 0};
+  int st = trsm_llu<C>(ctx, n, n, T, plain(Inv, ldi));
+  if (st) return st;
+  return trsm_lun<C>(ctx, n, n, T, plain(Inv, ldi));
 }
 
 // explicit instantiations
-template int gemm<double2>(const LaContext&, int, int, int, double2, const double2*, long long, const double2*,
-                           long long, double2, double2*, long long);
-template int getrf<double2>(const LaContext&, int, double2*, long long, int32_t*);
-template int getrf<float2>(const LaContext&, int, float2*, long long, int32_t*);
-template int solve_left<double2>(const LaContext&, int, int, const double2*, long long, const int32_t*, double2*,
-                                 long long);
-template int solve_left<float2>(const LaContext&, int, int, const float2*, long long, const int32_t*, float2*,
-                                long long);
-template int solve_right<double2>(const LaContext&, int, int, const double2*, long long, const int32_t*, double2*,
-                                  long long, double2*);
-template int solve_right<float2>(const LaContext&, int, int, const float2*, long long, const int32_t*, float2*,
-                                 long long, float2*);
-template int inverse<double2>(const LaContext&, int, const double2*, long long, const int32_t*, double2*, long long);
-template int inverse<float2>(const LaContext&, int, const float2*, long long, const int32_t*, float2*, long long);
+#define BEM_INST(C)                                                                                              \
+  template int gemm_v<C>(const LaContext&, int, int, int, C, RowView<C>, RowView<C>, C, RowView<C>);             \
+  template int getrf<C>(const LaContext&, int, C*, long long, int32_t*, int32_t*, int32_t*);                     \
+  template size_t solve_left_scratch_bytes<C>(int, int);                                                         \
+  template int solve_left<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long,     \
+                             void*);                                                                             \
+  template int solve_right<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long, C*); \
+  template int inverse<C>(const LaContext&, int, const C*, long long, const int32_t*, C*, long long);
+BEM_INST(double2)
+BEM_INST(float2)
 
 }  // namespace bem200
 
@@ -659,29 +1059,36 @@ size_t bem200_gemm_workspace_size(int engine, int m, int n, int k) {
   return gemm_tc_workspace(m, n, k, engine_of(engine));
 }
 
-int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* ipiv, int32_t* info, void* ws,
-                 size_t ws_bytes, void* stream) {
+int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv, int32_t* info,
+                 void* ws, size_t ws_bytes, void* stream) {
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
   ctx.engine = engine_of(engine);
   ctx.ws = ws;
   ctx.ws_bytes = ws_bytes;
   ctx.dinfo = info;
-  if (dtype == BEM200_C128) return getrf<double2>(ctx, n, (double2*)A, ld, ipiv);
-  if (dtype == BEM200_C64) return getrf<float2>(ctx, n, (float2*)A, ld, ipiv);
+  if (dtype == BEM200_C128) return getrf<double2>(ctx, n, (double2*)A, ld, rowmap, ipiv, nullptr);
+  if (dtype == BEM200_C64) return getrf<float2>(ctx, n, (float2*)A, ld, rowmap, ipiv, nullptr);
   set_error("getrf: bad dtype %d", dtype);
   return BEM200_ERR_ARG;
 }
 
-int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t ld, const int32_t* ipiv, void* B,
-                 int64_t ldb, void* ws, size_t ws_bytes, void* stream) {
+size_t bem200_getrs_workspace_size(int dtype, int n, int nrhs) {
+  return dtype == BEM200_C128 ? solve_left_scratch_bytes<double2>(n, nrhs) : solve_left_scratch_bytes<float2>(n, nrhs);
+}
+
+int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t ld, const int32_t* rowmap, void* B,
+                 int64_t ldb, void* ws, size_t ws_bytes, void* scratch, int32_t* status, void* stream) {
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
   ctx.engine = engine_of(engine);
   ctx.ws = ws;
   ctx.ws_bytes = ws_bytes;
-  if (dtype == BEM200_C128) return solve_left<double2>(ctx, n, nrhs, (const double2*)LU, ld, ipiv, (double2*)B, ldb);
-  if (dtype == BEM200_C64) return solve_left<float2>(ctx, n, nrhs, (const float2*)LU, ld, ipiv, (float2*)B, ldb);
+  ctx.dstatus = status;
+  if (dtype == BEM200_C128)
+    return solve_left<double2>(ctx, n, nrhs, (const double2*)LU, ld, rowmap, (double2*)B, ldb, scratch);
+  if (dtype == BEM200_C64)
+    return solve_left<float2>(ctx, n, nrhs, (const float2*)LU, ld, rowmap, (float2*)B, ldb, scratch);
   set_error("getrs: bad dtype %d", dtype);
   return BEM200_ERR_ARG;
 }

@@ -1,57 +1,100 @@
 // Dense complex linear algebra on one GPU (row-major, interleaved complex).
 //
-// Routines are host functions that enqueue kernels on a stream; recursion is
-// done on the host so that nearly all flops land in large GEMMs.
-//   getrf        : P A = L U with partial pivoting (LAPACK ipiv convention,
-//                  0-based global row indices)
-//   solve_left   : B <- A^-1 B   using the factors
-//   solve_right  : X <- X A^-1   using the factors (X A = Y)
-//   gemm         : C <- alpha A B + beta C
+// Factorisations use "lazy" row pivoting: rows are never moved while a
+// matrix is factored.  A factor is (storage, rowmap) where rowmap[i] is the
+// storage row holding logical row i of P A = L U.  All kernels address rows
+// through a RowView, so row exchanges cost nothing; LAPACK's ipiv (swap
+// sequence) is produced as well.
+//   getrf        : P A = L U with partial pivoting
+//   solve_left   : B <- A^-1 B     (blocked TRSV kernel for few right-hand sides)
+//   solve_right  : X <- X A^-1     (X A = Y)
+//   inverse      : A^-1
+//   gemm         : C <- alpha A B + beta C on row views
 // Element types: double2 (complex128, FP64 arithmetic) and float2 (complex64).
-// The complex64 GEMM runs on tcgen05 tensor cores when the tensor-core engine
-// is selected (see gemm_tc.cu), otherwise on CUDA cores.
+// The complex64 GEMM runs on tcgen05 tensor cores when a tensor-core engine
+// is selected (gemm_tc.cu), otherwise on CUDA cores.
 #pragma once
 #include "common.cuh"
 
 namespace bem200 {
 
 enum class GemmEngine : int {
-  kSimt = 0,       // CUDA-core FMA (FP64 for complex128, FP32 for complex64)
-  kTcBf16x3 = 1,   // complex64 on tcgen05: bf16 hi/lo split, 3 products, FP32 accumulate
-  kTcTf32 = 2,     // complex64 on tcgen05: TF32 inputs, FP32 accumulate
+  kSimt = 0,      // CUDA-core FMA (FP64 for complex128, FP32 for complex64)
+  kTcBf16x3 = 1,  // complex64 on tcgen05: bf16 hi/lo split, 3 products, FP32 accumulate
+  kTcTf32 = 2,    // complex64 on tcgen05: TF32 inputs, FP32 accumulate
 };
+
+// Row-addressed matrix view: element (i, j) lives at
+//   base[(map ? map[i] : i) * ld + col + j]
+// `map` already points at the first logical row of the view.
+template <typename C>
+struct RowView {
+  C* base;
+  long long ld;
+  const int32_t* map;
+  int col;
+  __host__ __device__ __forceinline__ long long off(int i, int j) const {
+    return (long long)(map ? map[i] : i) * ld + col + j;
+  }
+  __host__ __device__ __forceinline__ C& at(int i, int j) const { return base[off(i, j)]; }
+  // sub-view starting at logical row r, column c
+  __host__ __device__ __forceinline__ RowView sub(int r, int c) const {
+    RowView v = *this;
+    if (map) v.map = map + r; else v.base = base + (long long)r * ld;
+    v.col = col + c;
+    return v;
+  }
+};
+
+template <typename C>
+inline RowView<C> plain(C* p, long long ld) {
+  return RowView<C>{p, ld, nullptr, 0};
+}
 
 struct LaContext {
   cudaStream_t stream = nullptr;
   GemmEngine engine = GemmEngine::kSimt;
-  // scratch for the tensor-core operand preparation (bytes); may be null for kSimt
-  void* ws = nullptr;
+  void* ws = nullptr;  // scratch for the tensor-core operand preparation
   size_t ws_bytes = 0;
-  int* dinfo = nullptr;  // device int: first singular pivot (1-based) or 0
+  int* dinfo = nullptr;     // device int: first exactly-zero pivot (1-based) or 0
+  int* dstatus = nullptr;   // device int: set to a non-zero code if a bounded wait gave up
 };
 
 template <typename C>
-int gemm(const LaContext& ctx, int m, int n, int k, C alpha, const C* A, long long lda, const C* B,
-         long long ldb, C beta, C* Cm, long long ldc);
+int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv);
 
 template <typename C>
-int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* ipiv);
+inline int gemm(const LaContext& ctx, int m, int n, int k, C alpha, const C* A, long long lda, const C* B,
+                long long ldb, C beta, C* Cm, long long ldc) {
+  return gemm_v<C>(ctx, m, n, k, alpha, plain(const_cast<C*>(A), lda), plain(const_cast<C*>(B), ldb), beta,
+                   plain(Cm, ldc));
+}
 
+// P A = L U in place (storage rows stay put).  rowmap: n int32 (output),
+// ipiv: n int32 (output, LAPACK swap sequence, 0-based).  scratch: 4 n + 64 ints.
 template <typename C>
-int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld, const int32_t* ipiv, C* B,
-               long long ldb);
+int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv, int32_t* scratch);
 
+// B <- A^-1 B for the factor (LU, rowmap); B is n x nrhs (ldb).  scratch:
+// solve_left_scratch_bytes.
 template <typename C>
-int solve_right(const LaContext& ctx, int n, int m, const C* LU, long long ld, const int32_t* ipiv, C* X,
-                long long ldx, C* tmp /* m x n scratch, ld = n */);
+size_t solve_left_scratch_bytes(int n, int nrhs);
+template <typename C>
+int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld, const int32_t* rowmap, C* B,
+               long long ldb, void* scratch);
 
-// inverse of a factored matrix into Inv (n x n, ld ldi)
+// X <- X A^-1 (X is m x n); tmp: m x n elements.
 template <typename C>
-int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_t* ipiv, C* Inv, long long ldi);
+int solve_right(const LaContext& ctx, int n, int m, const C* LU, long long ld, const int32_t* rowmap, C* X,
+                long long ldx, C* tmp);
+
+// Inv <- A^-1 (n x n, ld ldi)
+template <typename C>
+int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_t* rowmap, C* Inv, long long ldi);
 
 // bytes of scratch the tensor-core GEMM needs for an m x n x k product
 size_t gemm_tc_workspace(int m, int n, int k, GemmEngine e);
-int gemm_tc_c64(const LaContext& ctx, int m, int n, int k, float2 alpha, const float2* A, long long lda,
-                const float2* B, long long ldb, float2 beta, float2* Cm, long long ldc);
+int gemm_tc_c64(const LaContext& ctx, int m, int n, int k, float2 alpha, RowView<float2> A, RowView<float2> B,
+                float2 beta, RowView<float2> Cv);
 
 }  // namespace bem200

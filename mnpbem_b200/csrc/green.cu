@@ -13,6 +13,9 @@
 //   region connectivity     mnpbem/greenfun/compgreen_ret.py:435-505, :739-858
 #include <cstdarg>
 #include <cmath>
+#include <atomic>
+#include <mutex>
+#include <unordered_map>
 
 #include "common.cuh"
 
@@ -27,6 +30,24 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 const char* get_error() { return g_err; }
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+cudaError_t set_kernel_attrs(const void* kern, int smem_bytes, bool nonportable_cluster) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> done;  // kernel -> largest smem limit set
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = done.find(kern);
+  if (it != done.end() && it->second >= smem_bytes) return cudaSuccess;
+  cudaError_t e = cudaSuccess;
+  if (smem_bytes > 0) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  if (e == cudaSuccess && nonportable_cluster)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e == cudaSuccess) done[kern] = smem_bytes;
+  return e;
+}
 
 constexpr int kMaxOrder = 7;
 constexpr double kEps = 2.220446049250313e-16;  // numpy finfo(float).eps
@@ -633,6 +654,8 @@ using namespace bem200;
 extern "C" {
 
 int bem200_version(void) { return 100; }
+
+uint64_t bem200_launch_count(void) { return (uint64_t)launch_count(); }
 
 int bem200_last_error(char* buf, size_t len) {
   const char* m = get_error();

@@ -59,7 +59,7 @@ def test_fp64_multi_polarisation(cuda):
     assert rel(sig.h2, ref["h2"]) < 1e-9
 
 
-@pytest.mark.parametrize("engine", ["simt"])
+@pytest.mark.parametrize("engine", ["simt", "bf16x3"])
 def test_mixed_ir_matches_fp64(cuda, engine):
     cp = dimer()
     _, sig64, ext64, sca64 = _run(cp, 620.0)

@@ -24,33 +24,46 @@ def getrf(A, engine=0):
     import torch
     n = A.shape[0]
     code = nat.C128 if A.dtype == torch.complex128 else nat.C64
+    rowmap = torch.empty(n, dtype=torch.int32, device="cuda")
     ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
     info = torch.zeros(1, dtype=torch.int32, device="cuda")
-    nat.call("bem200_getrf", code, engine, n, nat.ptr(A), n, nat.ptr(ipiv), nat.ptr(info), None, 0,
-             nat.stream_ptr())
-    return ipiv, info
+    nat.call("bem200_getrf", code, engine, n, nat.ptr(A), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info), None,
+             0, nat.stream_ptr())
+    return rowmap, ipiv, info
+
+
+def getrs(LU, rowmap, B):
+    import torch
+    n, nrhs = B.shape
+    code = nat.C128 if B.dtype == torch.complex128 else nat.C64
+    scr = torch.empty(int(nat.lib().bem200_getrs_workspace_size(code, n, nrhs)), dtype=torch.uint8, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    nat.call("bem200_getrs", code, 0, n, nrhs, nat.ptr(LU), n, nat.ptr(rowmap), nat.ptr(B), nrhs, None, 0,
+             nat.ptr(scr), nat.ptr(status), nat.stream_ptr())
+    assert int(status.item()) == 0
 
 
 @pytest.mark.parametrize("n", [33, 300, 1100])
 def test_getrf_c128_matches_lapack(cuda, n):
     A = _rand(n, n, n)
     At = _t(A)
-    ipiv, info = getrf(At)
+    rowmap, ipiv, info = getrf(At)
     lu, piv = sla.lu_factor(A)
     assert int(info.item()) == 0
     np.testing.assert_array_equal(ipiv.cpu().numpy(), piv)
-    err = np.max(np.abs(At.cpu().numpy() - lu)) / np.max(np.abs(lu))
+    # storage rows are not moved: logical row i lives in storage row rowmap[i]
+    got = At.cpu().numpy()[rowmap.cpu().numpy()]
+    err = np.max(np.abs(got - lu)) / np.max(np.abs(lu))
     assert err < 1e-11
 
 
-@pytest.mark.parametrize("n,nrhs", [(300, 1), (700, 5), (1100, 1100)])
+@pytest.mark.parametrize("n,nrhs", [(300, 1), (700, 5), (1000, 16), (1100, 1100), (77, 3)])
 def test_getrs_c128(cuda, n, nrhs):
     A = _rand(n, n, 7)
     B = _rand(n, nrhs, 8)
     At, Bt = _t(A), _t(B)
-    ipiv, _ = getrf(At)
-    nat.call("bem200_getrs", nat.C128, 0, n, nrhs, nat.ptr(At), n, nat.ptr(ipiv), nat.ptr(Bt), nrhs, None, 0,
-             nat.stream_ptr())
+    rowmap, _, _ = getrf(At)
+    getrs(At, rowmap, Bt)
     X = np.linalg.solve(A, B)
     assert np.max(np.abs(Bt.cpu().numpy() - X)) / np.max(np.abs(X)) < 1e-10
 
@@ -59,11 +72,10 @@ def test_getrf_c64(cuda):
     n = 900
     A = _rand(n, n, 3)
     At = _t(A.astype(np.complex64))
-    ipiv, info = getrf(At)
+    rowmap, ipiv, info = getrf(At)
     B = _rand(n, 4, 4)
     Bt = _t(B.astype(np.complex64))
-    nat.call("bem200_getrs", nat.C64, 0, n, 4, nat.ptr(At), n, nat.ptr(ipiv), nat.ptr(Bt), 4, None, 0,
-             nat.stream_ptr())
+    getrs(At, rowmap, Bt)
     X = np.linalg.solve(A, B)
     assert np.max(np.abs(Bt.cpu().numpy() - X)) / np.max(np.abs(X)) < 1e-3
 
@@ -86,5 +98,5 @@ def test_singular_pivot_reported(cuda):
     A = _rand(64, 64, 5)
     A[:, 10] = 0
     At = _t(A)
-    _, info = getrf(At)
+    _, _, info = getrf(At)
     assert int(info.item()) == 11
