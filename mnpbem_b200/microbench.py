@@ -1,0 +1,153 @@
+"""Single-stage timing and profiling cases of the retarded BEM solve.
+
+    python -m mnpbem_b200.microbench step  [--faces 1444] [--precision mixed|fp64] [--steps 1] [--warmup 1]
+    python -m mnpbem_b200.microbench green [--faces 1444] [--dtype c128|c64] [--reps 3]
+    python -m mnpbem_b200.microbench gemm  [--m 5768 --n 2884 --k 2884] [--engine 1] [--reps 3]
+    python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1]
+
+``step`` runs whole per-wavelength solves (assembly + init + solve) of the
+sphere dimer (two trisphere(faces) spheres, 2 nm gap, water, Drude gold,
+x-polarised plane wave along +z); the other cases run one library entry point
+on seeded inputs.  Each prints one JSON line with the CUDA-event time per
+call.  These small cases are what the kernel profiles are taken on.
+"""
+import argparse
+import ctypes
+import json
+import sys
+
+import numpy as np
+
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _timed(fn, reps):
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def dimer(faces=1444, diameter=40.0, gap=2.0):
+    from . import ComParticle, EpsConst, EpsDrude, trisphere
+    a, b = trisphere(faces, diameter), trisphere(faces, diameter)
+    a.shift([-(diameter / 2 + gap / 2), 0, 0])
+    b.shift([diameter / 2 + gap / 2, 0, 0])
+    return ComParticle([EpsConst(1.77), EpsDrude(9.84, 9.0, 0.067)], [a, b], [[2, 1], [2, 1]], 1, 2, interp="curv")
+
+
+def case_step(a):
+    import torch
+    from . import PlaneWaveRet
+    from .bem import BEMRet
+    cp = dimer(a.faces)
+    exc = PlaneWaveRet(np.array([[1.0, 0, 0]]), np.array([[0, 0, 1.0]]))
+    bem = BEMRet(cp, precision=a.precision, engine=a.engine)
+    b, npol = bem.rhs(exc.potential(cp, 650.0))
+    bt = torch.as_tensor(b, dtype=torch.complex128, device="cuda")
+
+    def one():
+        bem.clear()
+        bem.init(650.0)
+        bem.solve_device(bt, npol)
+    for _ in range(a.warmup):
+        one()
+    ms = _timed(one, a.steps)
+    return {"case": "step", "faces": cp.n, "precision": a.precision, "ms_per_step": ms, "ir": bem.last_ir}
+
+
+def case_green(a):
+    import torch
+    from .greenfun import CompGreenRet
+    cp = dimer(a.faces)
+    g = CompGreenRet(cp, cp)
+    n = cp.n
+    dt = torch.complex128 if a.dtype == "c128" else torch.complex64
+    out = [torch.empty((n, n), dtype=dt, device="cuda") for _ in range(4)]
+    g.bem_matrices(650.0, dtype=a.dtype, out=out)
+    ms = _timed(lambda: g.bem_matrices(650.0, dtype=a.dtype, out=out), a.reps)
+    nbytes = 4 * n * n * (16 if a.dtype == "c128" else 8)
+    return {"case": "green", "faces": n, "dtype": a.dtype, "ms": ms, "write_GBps": nbytes / ms / 1e6,
+            "nref": g.refined.nref}
+
+
+def case_gemm(a):
+    import torch
+    from . import _native as nat
+    m, n, k = a.m, a.n, a.k
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn(m, k, dtype=torch.complex64, device="cuda", generator=gen)
+    B = torch.randn(k, n, dtype=torch.complex64, device="cuda", generator=gen)
+    C = torch.zeros(m, n, dtype=torch.complex64, device="cuda")
+    wsb = int(nat.lib().bem200_gemm_workspace_size(a.engine, m, n, k))
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+    one = (ctypes.c_double * 2)(1.0, 0.0)
+    zero = (ctypes.c_double * 2)(0.0, 0.0)
+
+    def go():
+        nat.call("bem200_gemm", nat.C64, a.engine, m, n, k, one, nat.ptr(A), k, nat.ptr(B), n, zero, nat.ptr(C), n,
+                 nat.ptr(ws), wsb, nat.stream_ptr())
+    go()
+    ms = _timed(go, a.reps)
+    return {"case": "gemm", "m": m, "n": n, "k": k, "engine": a.engine, "ms": ms,
+            "complex_TFLOPs": 8.0 * m * n * k / ms / 1e9}
+
+
+def case_getrf(a):
+    import torch
+    from . import _native as nat
+    n = a.n
+    dt = torch.complex128 if a.dtype == "c128" else torch.complex64
+    code = nat.C128 if a.dtype == "c128" else nat.C64
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    A0 = torch.randn(n, n, dtype=dt, device="cuda", generator=gen)
+    A = torch.empty_like(A0)
+    rowmap = torch.empty(n, dtype=torch.int32, device="cuda")
+    ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    wsb = int(nat.lib().bem200_gemm_workspace_size(a.engine, n, n, n))
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+
+    def go():
+        A.copy_(A0)
+        nat.call("bem200_getrf", code, a.engine, n, nat.ptr(A), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info),
+                 nat.ptr(ws), wsb, nat.stream_ptr())
+    go()
+    ms = _timed(go, a.reps)
+    return {"case": "getrf", "n": n, "dtype": a.dtype, "engine": a.engine, "ms": ms,
+            "TFLOPs": 8.0 / 3.0 * n ** 3 / ms / 1e9, "info": int(info.item())}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["step", "green", "gemm", "getrf"])
+    ap.add_argument("--faces", type=int, default=1444)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--engine", type=int, default=1)
+    ap.add_argument("--dtype", default="c128", choices=["c128", "c64"])
+    ap.add_argument("--m", type=int, default=5768)
+    ap.add_argument("--n", type=int, default=2884)
+    ap.add_argument("--k", type=int, default=2884)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args(argv)
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("microbench needs a CUDA device")
+    if a.case == "step":
+        a.engine = {0: "simt", 1: "bf16x3", 2: "tf32"}[a.engine]
+    out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf}[a.case](a)
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
