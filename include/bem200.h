@@ -152,6 +152,21 @@ size_t bem200_getrs_workspace_size(int dtype, int n, int nrhs);
 int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t ld, const int32_t* rowmap,
                  void* B, int64_t ldb, void* ws, size_t ws_bytes, void* scratch, int32_t* status,
                  void* stream);
+/* Same solve as bem200_getrs (CUDA-core engine), for callers that cannot
+ * allocate device memory: a host program linking only this library with no
+ * device allocator of its own, or a caller whose device memory belongs to
+ * another runtime's pool and which must not call cudaMalloc / cudaFree
+ * (they synchronise the whole device).  No counterpart in the reference.
+ * The scratch comes from one fixed buffer of BEM200_GETRS_NOALLOC_MAX_BYTES
+ * in the library's device image (held by every GPU that loads the library
+ * until exit); sizes whose scratch (bem200_getrs_workspace_size) is larger
+ * are rejected with BEM200_ERR_ARG.  The call allocates nothing.  The first
+ * call on a device looks up the buffer's device address (host set-up); make
+ * it before any stream capture.  All calls on a GPU share the buffer: calls
+ * that overlap on the GPU race, so order them (one stream, or events). */
+#define BEM200_GETRS_NOALLOC_MAX_BYTES (4u << 20)
+int bem200_getrs_noalloc(int dtype, int n, int nrhs, const void* LU, int64_t ld, const int32_t* rowmap, void* B,
+                         int64_t ldb, int32_t* status, void* stream);
 
 /* ------------------------------------------------------------- dense BEM
  * precision 0 = complex128 throughout (the drop-in FP64 path);

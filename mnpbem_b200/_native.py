@@ -47,6 +47,8 @@ _SIGS = {
     "bem200_getrs_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "bem200_getrs": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _i64, _vp, _vp,
                                     _i64, _vp, _sz, _vp, _vp, _vp]),
+    "bem200_getrs_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _i64, _vp, _vp, _i64,
+                                            _vp, _vp]),
     "bem200_bem_status": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "bem200_bem_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int]),
     "bem200_bem_slots": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
