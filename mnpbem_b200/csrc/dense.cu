@@ -112,9 +112,95 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C a
   }
 }
 
+// Skinny GEMM: C (m x w) = alpha A (m x k) B (k x w) + beta C for w <= W
+// right-hand columns, a matrix-times-few-vectors product bound by streaming A
+// once from HBM.  Warp g of a CTA owns RW rows; lane l handles k = l (mod 32)
+// of every 128-wide k chunk, whose B rows sit in shared memory (odd pitch),
+// and keeps RW x W complex partial sums that are reduced across the warp at
+// the end.
+template <typename C, int W, int RW>
+__global__ void __launch_bounds__(256) gemm_skinny_kernel(int m, int w, int k, C alpha, RowView<C> A, RowView<C> B,
+                                                          C beta, RowView<C> Cv) {
+  constexpr int KC = 128;
+  __shared__ C bs[KC][W + 1];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int row0 = (blockIdx.x * 8 + wid) * RW;
+  long long aoff[RW];
+#pragma unroll
+  for (int r = 0; r < RW; ++r) aoff[r] = (row0 + r < m) ? A.off(row0 + r, 0) : -1;
+  C acc[RW][W];
+#pragma unroll
+  for (int r = 0; r < RW; ++r)
+#pragma unroll
+    for (int q = 0; q < W; ++q) acc[r][q] = czero<C>();
+  for (int k0 = 0; k0 < k; k0 += KC) {
+    __syncthreads();
+    for (int idx = tid; idx < KC * W; idx += 256) {
+      const int kk = idx / W, q = idx % W;
+      bs[kk][q] = (k0 + kk < k && q < w) ? B.at(k0 + kk, q) : czero<C>();
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int j = 0; j < KC / 32; ++j) {
+      const int kk = lane + 32 * j;
+      const int kg = k0 + kk;
+      C a[RW];
+#pragma unroll
+      for (int r = 0; r < RW; ++r) a[r] = (aoff[r] >= 0 && kg < k) ? A.base[aoff[r] + kg] : czero<C>();
+#pragma unroll
+      for (int q = 0; q < W; ++q) {
+        const C b = bs[kk][q];
+#pragma unroll
+        for (int r = 0; r < RW; ++r) {
+          acc[r][q].x = fma(a[r].x, b.x, acc[r][q].x);
+          acc[r][q].x = fma(-a[r].y, b.y, acc[r][q].x);
+          acc[r][q].y = fma(a[r].x, b.y, acc[r][q].y);
+          acc[r][q].y = fma(a[r].y, b.x, acc[r][q].y);
+        }
+      }
+    }
+  }
+  const bool use_beta = (beta.x != 0 || beta.y != 0);
+#pragma unroll
+  for (int r = 0; r < RW; ++r) {
+    C mine = czero<C>();
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      C v = acc[r][q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+      }
+      if (lane == q) mine = v;
+    }
+    if (aoff[r] >= 0 && lane < w) {
+      C& out = Cv.at(row0 + r, lane);
+      C v = cmul(alpha, mine);
+      if (use_beta) v = cadd(v, cmul(beta, out));
+      out = v;
+    }
+  }
+}
+
+template <typename C, int W, int RW>
+static int gemm_skinny(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta,
+                       RowView<C> Cv) {
+  const int grid = ceil_div(m, 8 * RW);
+  gemm_skinny_kernel<C, W, RW><<<grid, 256, 0, ctx.stream>>>(m, n, k, alpha, A, B, beta, Cv);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
 template <typename C>
 int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv) {
   if (m <= 0 || n <= 0) return BEM200_OK;
+  if (n <= 16 && k >= 256) {
+    // rows per warp: keep the partial sums of a thread within ~128 registers
+    constexpr int kRw8 = sizeof(C) == 16 ? 2 : 4, kRw16 = sizeof(C) == 16 ? 1 : 2;
+    if (n <= 8) return gemm_skinny<C, 8, kRw8>(ctx, m, n, k, alpha, A, B, beta, Cv);
+    return gemm_skinny<C, 16, kRw16>(ctx, m, n, k, alpha, A, B, beta, Cv);
+  }
   if constexpr (sizeof(C) == 8) {
     if (ctx.engine != GemmEngine::kSimt && k >= 64 && m >= 128 && n >= 64)
       return gemm_tc_c64(ctx, m, n, k, alpha, A, B, beta, Cv);
@@ -765,19 +851,60 @@ static int trsm_rlu(const LaContext& ctx, int m, int nrows, RowView<C> T, RowVie
 // an atomic counter; it consumes the solution blocks it depends on as their
 // flags are set, then solves its diagonal block and publishes its flag.  A CTA
 // only waits on blocks whose tickets were drawn earlier, so every wait ends;
-// each wait is nonetheless bounded and reports BEM200_ERR_TIMEOUT in *status.
+// each wait is nonetheless bounded and reports BEM200_ERR_TIMEOUT in *status
+// (the block then still publishes its flag so that no other block waits long).
+//
+// The triangle tiles do not depend on the flags: each CTA streams its tiles
+// with cp.async into a double buffer, one tile ahead of the flag it waits for.
+// The diagonal block is solved by a column sweep: warp w handles right-hand
+// side q = w (mod 8), lane l keeps rows l and l + 32 in registers, and each
+// step broadcasts the finished x_r and updates the remaining rows (one
+// shuffle and one complex FMA per lane).  The upper solve multiplies by
+// reciprocals of the diagonal, computed in parallel before the sweep.
 constexpr int kTrsvBS = 64;
 constexpr int kTrsvMaxRhs = 16;
+constexpr int kTrsvPitch = kTrsvBS + 1;  // odd pitch: the sweep's column reads are bank-conflict free
 constexpr long long kSpinLimit = 1LL << 22;
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+template <int B>
+__device__ __forceinline__ void cp_async_elem(void* s, const void* g);
+template <>
+__device__ __forceinline__ void cp_async_elem<8>(void* s, const void* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(su32(s)), "l"(g) : "memory");
+}
+template <>
+__device__ __forceinline__ void cp_async_elem<16>(void* s, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(su32(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// tile rows [r0, r0 + rb) x columns [c0, c0 + cb) of T -> dst (64 x kTrsvPitch), zero padded
+template <typename C>
+__device__ __forceinline__ void trsv_load_tile(C* dst, const RowView<C>& T, int r0, int rb, int c0, int cb) {
+  for (int idx = threadIdx.x; idx < kTrsvBS * kTrsvBS; idx += blockDim.x) {
+    const int r = idx >> 6, c = idx & 63;
+    C* d = dst + r * kTrsvPitch + c;
+    if (r < rb && c < cb)
+      cp_async_elem<sizeof(C)>(d, T.base + T.off(r0 + r, c0 + c));
+    else
+      *d = czero<C>();
+  }
+}
 
 template <typename C, bool kLower>
 __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowView<C> T, C* __restrict__ X,
                                                           int* __restrict__ flags, int* __restrict__ ticket,
                                                           int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char trsv_smem[];
-  auto tile = reinterpret_cast<C(*)[kTrsvBS + 1]>(trsv_smem);                                  // 64 x 65
-  auto xs = reinterpret_cast<C(*)[kTrsvMaxRhs]>(trsv_smem + sizeof(C) * kTrsvBS * (kTrsvBS + 1));  // 64 x 16
-  auto xj = xs + kTrsvBS;                                                                      // 64 x 16
+  C* tiles = reinterpret_cast<C*>(trsv_smem);        // 2 x 64 x kTrsvPitch
+  C* xs = tiles + 2 * kTrsvBS * kTrsvPitch;           // 64 x 16: this block's x
+  C* xj = xs + kTrsvBS * kTrsvMaxRhs;                 // 64 x 16: a finished block's x
   __shared__ int sI, sabort;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nblk = ceil_div(n, kTrsvBS);
@@ -790,14 +917,30 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
   if (tk >= nblk) return;
   const int I = kLower ? tk : nblk - 1 - tk;
   const int r0 = I * kTrsvBS, rb = min(kTrsvBS, n - r0);
-  for (int idx = tid; idx < kTrsvBS * nrhs; idx += 256) {
-    int r = idx / nrhs, q = idx % nrhs;
-    xs[r][q] = (r < rb) ? X[(long long)(r0 + r) * nrhs + q] : czero<C>();
+  const int nsrc = tk;  // blocks this one depends on: I of them (lower) or nblk - 1 - I (upper)
+  auto src_block = [&](int s) { return kLower ? s : nblk - 1 - s; };
+  {  // tile 0: the first dependency, or the diagonal block
+    const int J = nsrc > 0 ? src_block(0) : I;
+    trsv_load_tile(tiles, T, r0, rb, J * kTrsvBS, min(kTrsvBS, n - J * kTrsvBS));
+    cp_async_commit();
   }
-  const int nsrc = kLower ? I : nblk - 1 - I;
-  for (int s = 0; s < nsrc; ++s) {
-    const int J = kLower ? s : nblk - 1 - s;
+  for (int idx = tid; idx < kTrsvBS * nrhs; idx += 256) {
+    const int r = idx / nrhs, q = idx % nrhs;
+    xs[r * kTrsvMaxRhs + q] = (r < rb) ? X[(long long)(r0 + r) * nrhs + q] : czero<C>();
+  }
+  // split of the 64-long dot products over S lanes so that all 256 threads work
+  const int S = nrhs == 1 ? 4 : (nrhs == 2 ? 2 : 1);
+  const int nout = kTrsvBS * nrhs;
+  int s = 0;
+  for (; s < nsrc; ++s) {
+    const int J = src_block(s);
     const int c0 = J * kTrsvBS, cb = min(kTrsvBS, n - c0);
+    {  // prefetch tile s + 1 (the next dependency or the diagonal block)
+      const int Jn = (s + 1 < nsrc) ? src_block(s + 1) : I;
+      trsv_load_tile(tiles + ((s + 1) & 1) * kTrsvBS * kTrsvPitch, T, r0, rb, Jn * kTrsvBS,
+                     min(kTrsvBS, n - Jn * kTrsvBS));
+      cp_async_commit();
+    }
     if (tid == 0) {
       long long spins = 0;
       while (atomicAdd(&flags[J], 0) == 0) {
@@ -806,67 +949,80 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
           sabort = 1;
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
       __threadfence();
     }
     __syncthreads();
     if (sabort) break;
     for (int idx = tid; idx < kTrsvBS * nrhs; idx += 256) {
-      int c = idx / nrhs, q = idx % nrhs;
-      xj[c][q] = (c < cb) ? __ldcg(reinterpret_cast<const C*>(X) + (long long)(c0 + c) * nrhs + q) : czero<C>();
+      const int c = idx / nrhs, q = idx % nrhs;
+      xj[c * kTrsvMaxRhs + q] =
+          (c < cb) ? __ldcg(reinterpret_cast<const C*>(X) + (long long)(c0 + c) * nrhs + q) : czero<C>();
     }
-    for (int idx = tid; idx < rb * kTrsvBS; idx += 256) {
-      int r = idx >> 6, c = idx & 63;
-      tile[r][c] = (c < cb) ? T.at(r0 + r, c0 + c) : czero<C>();
+    cp_async_wait<1>();  // tile s has landed; tile s + 1 may still be in flight
+    __syncthreads();
+    const C* tile = tiles + (s & 1) * kTrsvBS * kTrsvPitch;
+    for (int base = 0; base < nout * S; base += 256) {
+      const int idx = base + tid;
+      const int o = idx / S, part = idx % S;
+      C acc = czero<C>();
+      if (o < nout) {
+        const int r = o / nrhs, q = o % nrhs;
+        const C* trow = tile + r * kTrsvPitch;
+#pragma unroll 8
+        for (int c = part; c < kTrsvBS; c += S) acc = cadd(acc, cmul(trow[c], xj[c * kTrsvMaxRhs + q]));
+      }
+      for (int off = 1; off < S; off <<= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+      }
+      if (o < nout && part == 0) {
+        const int r = o / nrhs, q = o % nrhs;
+        xs[r * kTrsvMaxRhs + q] = csub(xs[r * kTrsvMaxRhs + q], acc);
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  if (!sabort) {
+    const C* D = tiles + (nsrc & 1) * kTrsvBS * kTrsvPitch;  // the diagonal block
+    for (int q = wid; q < nrhs; q += 8) {
+      C x0 = xs[lane * kTrsvMaxRhs + q], x1 = xs[(lane + 32) * kTrsvMaxRhs + q];
+      const C* d0 = D + lane * kTrsvPitch;
+      const C* d1 = D + (lane + 32) * kTrsvPitch;
+      if (kLower) {
+        for (int r = 0; r < rb; ++r) {
+          const C xr = shfl_c(r < 32 ? x0 : x1, r & 31);
+          const C u0 = csub(x0, cmul(d0[r], xr)), u1 = csub(x1, cmul(d1[r], xr));
+          if (lane > r) x0 = u0;
+          if (lane + 32 > r) x1 = u1;
+        }
+      } else {
+        const C one = cmake<C>(1.0, 0.0);
+        const C inv0 = lane < rb ? cdiv(one, d0[lane]) : czero<C>();
+        const C inv1 = lane + 32 < rb ? cdiv(one, d1[lane + 32]) : czero<C>();
+        for (int r = rb - 1; r >= 0; --r) {
+          if (r < 32) {
+            if (lane == r) x0 = cmul(x0, inv0);
+          } else if (lane == r - 32) {
+            x1 = cmul(x1, inv1);
+          }
+          const C xr = shfl_c(r < 32 ? x0 : x1, r & 31);
+          const C u0 = csub(x0, cmul(d0[r], xr)), u1 = csub(x1, cmul(d1[r], xr));
+          if (lane < r) x0 = u0;
+          if (lane + 32 < r) x1 = u1;
+        }
+      }
+      xs[lane * kTrsvMaxRhs + q] = x0;
+      xs[(lane + 32) * kTrsvMaxRhs + q] = x1;
     }
     __syncthreads();
     for (int idx = tid; idx < rb * nrhs; idx += 256) {
-      int r = idx / nrhs, q = idx % nrhs;
-      C acc = xs[r][q];
-      for (int c = 0; c < cb; ++c) acc = csub(acc, cmul(tile[r][c], xj[c][q]));
-      xs[r][q] = acc;
+      const int r = idx / nrhs, q = idx % nrhs;
+      X[(long long)(r0 + r) * nrhs + q] = xs[r * kTrsvMaxRhs + q];
     }
-    __syncthreads();
-  }
-  // diagonal block
-  for (int idx = tid; idx < rb * kTrsvBS; idx += 256) {
-    int r = idx >> 6, c = idx & 63;
-    tile[r][c] = (c < rb) ? T.at(r0 + r, r0 + c) : czero<C>();
-  }
-  __syncthreads();
-  // warp q solves right-hand side q; lanes split the dot products
-  for (int q = wid; q < nrhs; q += 8) {
-    if (kLower) {
-      for (int r = 0; r < rb; ++r) {
-        C part = czero<C>();
-        for (int c = lane; c < r; c += 32) part = cadd(part, cmul(tile[r][c], xs[c][q]));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          part.x += __shfl_xor_sync(0xffffffffu, part.x, o);
-          part.y += __shfl_xor_sync(0xffffffffu, part.y, o);
-        }
-        if (lane == 0) xs[r][q] = csub(xs[r][q], part);
-        __syncwarp();
-      }
-    } else {
-      for (int r = rb - 1; r >= 0; --r) {
-        C part = czero<C>();
-        for (int c = r + 1 + lane; c < rb; c += 32) part = cadd(part, cmul(tile[r][c], xs[c][q]));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          part.x += __shfl_xor_sync(0xffffffffu, part.x, o);
-          part.y += __shfl_xor_sync(0xffffffffu, part.y, o);
-        }
-        if (lane == 0) xs[r][q] = cdiv(csub(xs[r][q], part), tile[r][r]);
-        __syncwarp();
-      }
-    }
-  }
-  __syncthreads();
-  for (int idx = tid; idx < rb * nrhs; idx += 256) {
-    int r = idx / nrhs, q = idx % nrhs;
-    X[(long long)(r0 + r) * nrhs + q] = xs[r][q];
   }
   __threadfence();
   __syncthreads();
@@ -875,7 +1031,7 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
 
 template <typename C>
 static size_t trsv_smem_bytes() {
-  return sizeof(C) * (kTrsvBS * (kTrsvBS + 1) + 2 * kTrsvBS * kTrsvMaxRhs);
+  return sizeof(C) * (2 * kTrsvBS * kTrsvPitch + 2 * kTrsvBS * kTrsvMaxRhs);
 }
 
 template <typename C, bool kLower>

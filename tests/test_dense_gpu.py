@@ -100,3 +100,19 @@ def test_singular_pivot_reported(cuda):
     At = _t(A)
     _, _, info = getrf(At)
     assert int(info.item()) == 11
+
+
+@pytest.mark.parametrize("dt,tol", [(np.complex128, 1e-13), (np.complex64, 1e-5)])
+@pytest.mark.parametrize("n", [1, 4, 8, 12, 16])
+def test_gemm_skinny(cuda, dt, tol, n):
+    """Matrix times few vectors (n <= 16, k >= 256): the bandwidth-bound skinny kernel."""
+    m, k = 1000, 700
+    A, B, C = _rand(m, k, 11, dt), _rand(k, n, 12, dt), _rand(m, n, 13, dt)
+    At, Bt, Ct = _t(A), _t(B), _t(C)
+    alpha = (ctypes.c_double * 2)(1.5, 0.5)
+    beta = (ctypes.c_double * 2)(-0.5, 2.0)
+    code = nat.C128 if dt == np.complex128 else nat.C64
+    nat.call("bem200_gemm", code, 0, m, n, k, alpha, nat.ptr(At), k, nat.ptr(Bt), n, beta, nat.ptr(Ct), n, None, 0,
+             nat.stream_ptr())
+    ref = (1.5 + 0.5j) * (A.astype(np.complex128) @ B) + (-0.5 + 2j) * C
+    assert np.max(np.abs(Ct.cpu().numpy() - ref)) / np.max(np.abs(ref)) < tol
