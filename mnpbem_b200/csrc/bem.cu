@@ -101,6 +101,21 @@ __global__ void sigma_kernel(int n, const C* __restrict__ S1, const C* __restric
   S[idx] = to_c<C>(v);
 }
 
+// The factor chains of G1 and G2 are independent: LU(G2) and Sigma2 run on a
+// second (non-blocking) stream forked from the caller's stream with events, so
+// the latency-bound panel factorisations of the two chains overlap.  Each
+// chain gets its own half of the tensor-core operand workspace; Sigma2 uses
+// the Delta slot (free until the join) as its scratch matrix.
+struct ForkJoin {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  ~ForkJoin() {
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (side) cudaStreamDestroy(side);  // released once its queued work has finished
+  }
+};
+
 template <typename C>
 static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, const double* nvec, double k0) {
   BemState<C> s = state_view<C>(n, ws);
@@ -110,12 +125,38 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
   c.dstatus = s.status;
   BEM_CUDA_CHECK(cudaMemsetAsync(s.info, 0, 2 * sizeof(int), ctx.stream));
   int st;
-  // LU(G1), LU(G2)
+  // a second chain needs half of the operand workspace for the largest GEMM of
+  // an LU / right solve (n x n/2 x n/2, rounded up)
+  const int half = n / 2 + 64;
+  const bool split_ws = ctx.engine != GemmEngine::kSimt;
+  const bool fork = !split_ws || gemm_tc_workspace(n, half, half, ctx.engine) <= ctx.ws_bytes / 2;
+  ForkJoin fj;
+  LaContext c2 = c;
+  if (fork) {
+    BEM_CUDA_CHECK(cudaStreamCreateWithFlags(&fj.side, cudaStreamNonBlocking));
+    BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fj.fork, cudaEventDisableTiming));
+    BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fj.join, cudaEventDisableTiming));
+    BEM_CUDA_CHECK(cudaEventRecord(fj.fork, ctx.stream));
+    BEM_CUDA_CHECK(cudaStreamWaitEvent(fj.side, fj.fork, 0));
+    c2.stream = fj.side;
+    if (split_ws) {
+      const size_t h = (ctx.ws_bytes / 2) & ~size_t(255);
+      c.ws_bytes = h;
+      c2.ws = reinterpret_cast<char*>(ctx.ws) + h;
+      c2.ws_bytes = h;
+    }
+  }
+  // chain 1: LU(G1), Sigma1 = H1 G1^-1 (M5 is scratch)
   if ((st = getrf<C>(c, n, s.M[0], n, s.map[0], s.ipiv[0], nullptr))) return st;
-  if ((st = getrf<C>(c, n, s.M[1], n, s.map[1], s.ipiv[1], nullptr))) return st;
-  // Sigma1 = H1 G1^-1, Sigma2 = H2 G2^-1 (right solves; M5 is scratch)
+  // chain 2: LU(G2), Sigma2 = H2 G2^-1 (M4 is scratch)
+  if ((st = getrf<C>(c2, n, s.M[1], n, s.map[1], s.ipiv[1], nullptr))) return st;
   if ((st = solve_right<C>(c, n, n, s.M[0], n, s.map[0], s.M[2], n, s.M[5]))) return st;
-  if ((st = solve_right<C>(c, n, n, s.M[1], n, s.map[1], s.M[3], n, s.M[5]))) return st;
+  if ((st = solve_right<C>(c2, n, n, s.M[1], n, s.map[1], s.M[3], n, fork ? s.M[4] : s.M[5]))) return st;
+  if (fork) {
+    BEM_CUDA_CHECK(cudaEventRecord(fj.join, fj.side));
+    BEM_CUDA_CHECK(cudaStreamWaitEvent(ctx.stream, fj.join, 0));
+    c.ws_bytes = ctx.ws_bytes;
+  }
   // Delta = Sigma1 - Sigma2, LU(Delta), Delta^-1
   delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[4]);
   BEM_LAUNCH_CHECK();

@@ -665,89 +665,118 @@ static int panel_lu(const LaContext& ctx, int m, int w, C* A, long long ld, int 
 }
 
 // ===================================================================== TRSM leaves
-// Blocks of 128 threads; each thread owns one right-hand side (a column of B for
-// left solves, a row of X for right solves).  The triangle (m <= 32) and the
-// right-hand sides live in shared memory.
-constexpr int kTrsmNB = 32;
-constexpr int kTrsmThreads = 128;
+// A leaf solves with a triangle of m <= NB rows (NB = 128 for complex64, 64 for
+// complex128) held in shared memory (odd pitch).  Each warp sweeps one
+// right-hand vector at a time -- a column of B for left solves, a row of X for
+// right solves.  Lane l holds elements l + 32 t of the vector in registers;
+// each step of the sweep finishes one element, broadcasts it with a shuffle and
+// updates the elements still open (NB / 32 complex FMAs per lane at most).
+// Divisions by the diagonal use reciprocals computed before the sweep.  A CTA
+// owns kLeafVecs vectors, two per warp.
+template <typename C> struct LeafNB { static constexpr int value = 128; };
+template <> struct LeafNB<double2> { static constexpr int value = 64; };
+constexpr int kLeafThreads = 256;
+constexpr int kLeafVecs = 16;
 
-// B[0:m, c] <- T^-1 B[0:m, c]; lower = unit lower (L), else upper non-unit (U)
-template <typename C, bool kLower>
-__global__ void __launch_bounds__(kTrsmThreads) trsm_left_leaf(int m, int ncols, RowView<C> T, RowView<C> B) {
-  extern __shared__ __align__(16) unsigned char trsm_smem[];
-  auto Ts = reinterpret_cast<C(*)[kTrsmNB + 1]>(trsm_smem);
-  auto Bs = reinterpret_cast<C(*)[kTrsmThreads]>(trsm_smem + sizeof(C) * kTrsmNB * (kTrsmNB + 1));
-  const int c0 = blockIdx.x * kTrsmThreads;
-  for (int idx = threadIdx.x; idx < m * m; idx += kTrsmThreads) {
-    int r = idx / m, c = idx % m;
-    Ts[r][c] = T.at(r, c);
+enum LeafKind : int {
+  kLeftLowerUnit = 0,   // B <- L^-1 B
+  kLeftUpper = 1,       // B <- U^-1 B
+  kRightUpper = 2,      // X <- X U^-1
+  kRightLowerUnit = 3,  // X <- X L^-1
+};
+
+template <typename C, int K>
+__global__ void __launch_bounds__(kLeafThreads) trsm_leaf_kernel(int m, int nvec, RowView<C> T, RowView<C> B) {
+  constexpr int NB = LeafNB<C>::value, NT = NB / 32, P = NB + 1;
+  constexpr bool kLeft = (K == kLeftLowerUnit || K == kLeftUpper);
+  constexpr bool kForward = (K == kLeftLowerUnit || K == kRightUpper);
+  constexpr bool kUnit = (K == kLeftLowerUnit || K == kRightLowerUnit);
+  extern __shared__ __align__(16) unsigned char leaf_smem[];
+  C* Ts = reinterpret_cast<C*>(leaf_smem);  // NB x P triangle block
+  C* Vs = Ts + NB * P;                       // kLeafVecs x P: vector v, element e at Vs[v * P + e]
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int v0 = blockIdx.x * kLeafVecs;
+  const int nv = min(kLeafVecs, nvec - v0);
+  for (int idx = tid; idx < NB * NB; idx += kLeafThreads) {
+    const int r = idx / NB, c = idx % NB;
+    Ts[r * P + c] = (r < m && c < m) ? T.at(r, c) : czero<C>();
   }
-  for (int idx = threadIdx.x; idx < m * kTrsmThreads; idx += kTrsmThreads) {
-    int r = idx / kTrsmThreads, c = idx % kTrsmThreads;
-    Bs[r][c] = (c0 + c < ncols) ? B.at(r, c0 + c) : czero<C>();
-  }
-  __syncthreads();
-  const int c = threadIdx.x;
-  if (kLower) {
-    for (int r = 1; r < m; ++r) {
-      C s = Bs[r][c];
-      for (int q = 0; q < r; ++q) s = csub(s, cmul(Ts[r][q], Bs[q][c]));
-      Bs[r][c] = s;
+  if (kLeft) {
+    for (int idx = tid; idx < NB * kLeafVecs; idx += kLeafThreads) {
+      const int e = idx / kLeafVecs, v = idx % kLeafVecs;
+      if (v < nv) Vs[v * P + e] = (e < m) ? B.at(e, v0 + v) : czero<C>();
     }
   } else {
-    for (int r = m - 1; r >= 0; --r) {
-      C s = Bs[r][c];
-      for (int q = r + 1; q < m; ++q) s = csub(s, cmul(Ts[r][q], Bs[q][c]));
-      Bs[r][c] = cdiv(s, Ts[r][r]);
+    for (int idx = tid; idx < NB * kLeafVecs; idx += kLeafThreads) {
+      const int v = idx / NB, e = idx % NB;
+      if (v < nv) Vs[v * P + e] = (e < m) ? B.at(v0 + v, e) : czero<C>();
     }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < m * kTrsmThreads; idx += kTrsmThreads) {
-    int r = idx / kTrsmThreads, cc = idx % kTrsmThreads;
-    if (c0 + cc < ncols) B.at(r, c0 + cc) = Bs[r][cc];
-  }
-}
-
-// X[r, 0:m] <- X[r, 0:m] T^-1 ; upper = non-unit upper (U), else unit lower (L)
-template <typename C, bool kUpper>
-__global__ void __launch_bounds__(kTrsmThreads) trsm_right_leaf(int m, int nrows, RowView<C> T, RowView<C> X) {
-  extern __shared__ __align__(16) unsigned char trsm_smem[];
-  auto Ts = reinterpret_cast<C(*)[kTrsmNB + 1]>(trsm_smem);
-  auto Xs = reinterpret_cast<C(*)[kTrsmNB + 1]>(trsm_smem + sizeof(C) * kTrsmNB * (kTrsmNB + 1));
-  const int r0 = blockIdx.x * kTrsmThreads;
-  for (int idx = threadIdx.x; idx < m * m; idx += kTrsmThreads) {
-    int r = idx / m, c = idx % m;
-    Ts[r][c] = T.at(r, c);
-  }
-  for (int idx = threadIdx.x; idx < m * kTrsmThreads; idx += kTrsmThreads) {
-    int r = idx / m, c = idx % m;
-    Xs[r][c] = (r0 + r < nrows) ? X.at(r0 + r, c) : czero<C>();
+  for (int v = wid; v < nv; v += kLeafThreads / 32) {
+    C x[NT], inv[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int e = lane + 32 * t;
+      x[t] = Vs[v * P + e];
+      inv[t] = (!kUnit && e < m) ? cdiv(cmake<C>(1.0, 0.0), Ts[e * P + e]) : czero<C>();
+    }
+    if (kForward) {
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        for (int rr = 0; rr < 32; ++rr) {
+          const int r = 32 * t + rr;
+          if (r >= m) break;
+          if (!kUnit && lane == rr) x[t] = cmul(x[t], inv[t]);
+          const C xr = shfl_c(x[t], rr);
+#pragma unroll
+          for (int u = t; u < NT; ++u) {
+            const int e = lane + 32 * u;
+            const C coef = kLeft ? Ts[e * P + r] : Ts[r * P + e];
+            const C nx = csub(x[u], cmul(coef, xr));
+            if (e > r) x[u] = nx;
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int t = NT - 1; t >= 0; --t) {
+        for (int rr = 31; rr >= 0; --rr) {
+          const int r = 32 * t + rr;
+          if (r >= m) continue;
+          if (!kUnit && lane == rr) x[t] = cmul(x[t], inv[t]);
+          const C xr = shfl_c(x[t], rr);
+#pragma unroll
+          for (int u = 0; u <= t; ++u) {
+            const int e = lane + 32 * u;
+            const C coef = kLeft ? Ts[e * P + r] : Ts[r * P + e];
+            const C nx = csub(x[u], cmul(coef, xr));
+            if (e < r) x[u] = nx;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < NT; ++t) Vs[v * P + lane + 32 * t] = x[t];
   }
   __syncthreads();
-  const int r = threadIdx.x;
-  if (kUpper) {
-    for (int c = 0; c < m; ++c) {
-      C s = Xs[r][c];
-      for (int q = 0; q < c; ++q) s = csub(s, cmul(Xs[r][q], Ts[q][c]));
-      Xs[r][c] = cdiv(s, Ts[c][c]);
+  if (kLeft) {
+    for (int idx = tid; idx < NB * kLeafVecs; idx += kLeafThreads) {
+      const int e = idx / kLeafVecs, v = idx % kLeafVecs;
+      if (v < nv && e < m) B.at(e, v0 + v) = Vs[v * P + e];
     }
   } else {
-    for (int c = m - 1; c >= 0; --c) {
-      C s = Xs[r][c];
-      for (int q = c + 1; q < m; ++q) s = csub(s, cmul(Xs[r][q], Ts[q][c]));
-      Xs[r][c] = s;
+    for (int idx = tid; idx < NB * kLeafVecs; idx += kLeafThreads) {
+      const int v = idx / NB, e = idx % NB;
+      if (v < nv && e < m) B.at(v0 + v, e) = Vs[v * P + e];
     }
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < m * kTrsmThreads; idx += kTrsmThreads) {
-    int rr = idx / m, c = idx % m;
-    if (r0 + rr < nrows) X.at(r0 + rr, c) = Xs[rr][c];
   }
 }
 
 template <typename C>
-static size_t trsm_smem_bytes() {
-  return sizeof(C) * (kTrsmNB * (kTrsmNB + 1) + kTrsmThreads * (kTrsmNB + 1));
+static size_t leaf_smem_bytes() {
+  constexpr int NB = LeafNB<C>::value;
+  return sizeof(C) * (size_t)(NB + kLeafVecs) * (NB + 1);
 }
 
 template <typename K>
@@ -756,28 +785,33 @@ static int prep_smem(K kern, size_t bytes) {
   return BEM200_OK;
 }
 
+template <typename C, int K>
+static int trsm_leaf(const LaContext& ctx, int m, int nvec, RowView<C> T, RowView<C> B) {
+  auto kern = trsm_leaf_kernel<C, K>;
+  int st = prep_smem(kern, leaf_smem_bytes<C>());
+  if (st) return st;
+  kern<<<ceil_div(nvec, kLeafVecs), kLeafThreads, leaf_smem_bytes<C>(), ctx.stream>>>(m, nvec, T, B);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
 template <typename C> static C neg_one() { return cmake<C>(-1.0, 0.0); }
 template <typename C> static C one() { return cmake<C>(1.0, 0.0); }
 
-static int split_point(int m) {
+// split of m rows for a recursion on multiples of q (both parts non-empty)
+static int split_point(int m, int q) {
   int h = m / 2;
-  h = ((h + kTrsmNB - 1) / kTrsmNB) * kTrsmNB;
-  return h < m ? h : m - kTrsmNB;
+  h = ((h + q - 1) / q) * q;
+  return h < m ? h : m - q;
 }
 
 // B <- L^-1 B, L unit lower m x m (strict lower part of T)
 template <typename C>
 static int trsm_llu(const LaContext& ctx, int m, int ncols, RowView<C> T, RowView<C> B) {
+  constexpr int NB = LeafNB<C>::value;
   if (m <= 0 || ncols <= 0) return BEM200_OK;
-  if (m <= kTrsmNB) {
-    int st = prep_smem(trsm_left_leaf<C, true>, trsm_smem_bytes<C>());
-    if (st) return st;
-    trsm_left_leaf<C, true><<<ceil_div(ncols, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(
-        m, ncols, T, B);
-    BEM_LAUNCH_CHECK();
-    return BEM200_OK;
-  }
-  int m1 = split_point(m);
+  if (m <= NB) return trsm_leaf<C, kLeftLowerUnit>(ctx, m, ncols, T, B);
+  int m1 = split_point(m, NB);
   int st = trsm_llu(ctx, m1, ncols, T, B);
   if (st) return st;
   st = gemm_v<C>(ctx, m - m1, ncols, m1, neg_one<C>(), T.sub(m1, 0), B, one<C>(), B.sub(m1, 0));
@@ -788,16 +822,10 @@ static int trsm_llu(const LaContext& ctx, int m, int ncols, RowView<C> T, RowVie
 // B <- U^-1 B, U upper non-unit
 template <typename C>
 static int trsm_lun(const LaContext& ctx, int m, int ncols, RowView<C> T, RowView<C> B) {
+  constexpr int NB = LeafNB<C>::value;
   if (m <= 0 || ncols <= 0) return BEM200_OK;
-  if (m <= kTrsmNB) {
-    int st = prep_smem(trsm_left_leaf<C, false>, trsm_smem_bytes<C>());
-    if (st) return st;
-    trsm_left_leaf<C, false><<<ceil_div(ncols, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(
-        m, ncols, T, B);
-    BEM_LAUNCH_CHECK();
-    return BEM200_OK;
-  }
-  int m1 = split_point(m);
+  if (m <= NB) return trsm_leaf<C, kLeftUpper>(ctx, m, ncols, T, B);
+  int m1 = split_point(m, NB);
   int st = trsm_lun(ctx, m - m1, ncols, T.sub(m1, m1), B.sub(m1, 0));
   if (st) return st;
   st = gemm_v<C>(ctx, m1, ncols, m - m1, neg_one<C>(), T.sub(0, m1), B.sub(m1, 0), one<C>(), B);
@@ -808,16 +836,10 @@ static int trsm_lun(const LaContext& ctx, int m, int ncols, RowView<C> T, RowVie
 // X <- X U^-1, X nrows x m
 template <typename C>
 static int trsm_run(const LaContext& ctx, int m, int nrows, RowView<C> T, RowView<C> X) {
+  constexpr int NB = LeafNB<C>::value;
   if (m <= 0 || nrows <= 0) return BEM200_OK;
-  if (m <= kTrsmNB) {
-    int st = prep_smem(trsm_right_leaf<C, true>, trsm_smem_bytes<C>());
-    if (st) return st;
-    trsm_right_leaf<C, true><<<ceil_div(nrows, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(
-        m, nrows, T, X);
-    BEM_LAUNCH_CHECK();
-    return BEM200_OK;
-  }
-  int m1 = split_point(m);
+  if (m <= NB) return trsm_leaf<C, kRightUpper>(ctx, m, nrows, T, X);
+  int m1 = split_point(m, NB);
   int st = trsm_run(ctx, m1, nrows, T, X);
   if (st) return st;
   st = gemm_v<C>(ctx, nrows, m - m1, m1, neg_one<C>(), X, T.sub(0, m1), one<C>(), X.sub(0, m1));
@@ -828,16 +850,10 @@ static int trsm_run(const LaContext& ctx, int m, int nrows, RowView<C> T, RowVie
 // X <- X L^-1, L unit lower
 template <typename C>
 static int trsm_rlu(const LaContext& ctx, int m, int nrows, RowView<C> T, RowView<C> X) {
+  constexpr int NB = LeafNB<C>::value;
   if (m <= 0 || nrows <= 0) return BEM200_OK;
-  if (m <= kTrsmNB) {
-    int st = prep_smem(trsm_right_leaf<C, false>, trsm_smem_bytes<C>());
-    if (st) return st;
-    trsm_right_leaf<C, false><<<ceil_div(nrows, kTrsmThreads), kTrsmThreads, trsm_smem_bytes<C>(), ctx.stream>>>(
-        m, nrows, T, X);
-    BEM_LAUNCH_CHECK();
-    return BEM200_OK;
-  }
-  int m1 = split_point(m);
+  if (m <= NB) return trsm_leaf<C, kRightLowerUnit>(ctx, m, nrows, T, X);
+  int m1 = split_point(m, NB);
   int st = trsm_rlu(ctx, m - m1, nrows, T.sub(m1, m1), X.sub(0, m1));
   if (st) return st;
   st = gemm_v<C>(ctx, nrows, m1, m - m1, neg_one<C>(), X.sub(0, m1), T.sub(m1, 0), one<C>(), X);
@@ -1058,7 +1074,7 @@ template <typename C>
 static int getrf_rec(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv, int col0,
                      int w) {
   if (w <= kPanelNB) return panel_lu<C>(ctx, n - col0, w, A, ld, col0, rowmap + col0, ipiv + col0, col0);
-  int w1 = split_point(w);
+  int w1 = split_point(w, kPanelNB);
   int st = getrf_rec(ctx, n, A, ld, rowmap, ipiv, col0, w1);
   if (st) return st;
   RowView<C> V{A, ld, rowmap + col0, col0};  // logical rows from col0, columns from col0
