@@ -612,9 +612,171 @@ __global__ void __launch_bounds__(kRegThreads, 1) panel_lu_reg_kernel(int m, int
   }
 }
 
+// ----------------------------------------------------------------------------
+// Push panel: one panel row per thread, held in registers (32 complex), with
+// the column loop fully unrolled so every register index is static.  Per
+// column: warp argmax -> the winning lane parks its row in shared memory ->
+// warp 0 picks the CTA's best row and PUSHES it (value, index, 32 elements)
+// into the candidate slot of every CTA of the cluster with DSMEM stores ->
+// one cluster barrier -> every warp reduces the cs candidates from its own
+// shared memory and applies the update with the winning row.  Nothing is read
+// remotely, so the barrier is the only cluster-wide latency per column.
+// Candidate slots are double buffered: slot t & 1 is rewritten at column t + 2,
+// after every CTA has passed barrier t + 1 and thus finished reading it.
+constexpr int kPushThreads = 384;
+constexpr int kPushWarps = kPushThreads / 32;
+constexpr int kPushMaxCluster = 16;
+
+template <typename C>
+struct PushShared {
+  C cand[2][kPushMaxCluster][kPanelNB];
+  R_t<C> cval[2][kPushMaxCluster];
+  int crow[2][kPushMaxCluster];
+  C wrow[kPushWarps][kPanelNB];
+  R_t<C> wval[kPushWarps];
+  int widx[kPushWarps];
+  int perm[kPanelNB];
+  int singular;
+};
+
+template <typename C>
+__global__ void __launch_bounds__(kPushThreads, 1) panel_lu_push_kernel(int m, int w, C* __restrict__ A, long long ld,
+                                                                        int col, int32_t* __restrict__ rowmap,
+                                                                        int32_t* __restrict__ ipiv, int ipiv_base,
+                                                                        int* __restrict__ info, int R) {
+  using Real = R_t<C>;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int cs = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  __shared__ PushShared<C> sh;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int r0 = rank * R;
+  const int rcount = max(0, min(R, m - r0));
+  const int prow_id = r0 + tid;  // panel row of this thread
+  bool act = tid < rcount;
+  const long long phys = act ? (long long)rowmap[prow_id] : 0;
+  C v[kPanelNB];
+#pragma unroll
+  for (int c = 0; c < kPanelNB; ++c) v[c] = (act && c < w) ? A[phys * ld + col + c] : czero<C>();
+  if (tid == 0) sh.singular = 0;
+  const unsigned kFull = 0xffffffffu;
+
+  // The column loop stays rolled (a fully unrolled one overflows the
+  // instruction cache); column t of the register row is read with a select
+  // chain and updated with predicated FMAs, so every register index is static.
+#pragma unroll 1
+  for (int t = 0; t < w; ++t) {
+    const int buf = t & 1;
+    C vt = v[0];
+#pragma unroll
+    for (int c = 1; c < kPanelNB; ++c)
+      if (c == t) vt = v[c];
+    // warp candidate; the winning lane parks its row in shared memory
+    Real wb = act ? pmag(vt) : (Real)-1;
+    int wi = act ? prow_id : INT_MAX;
+    warp_argmax<C>(wb, wi);
+    if (act && wi == prow_id) {
+#pragma unroll
+      for (int c = 0; c < kPanelNB; ++c) sh.wrow[wid][c] = v[c];
+    }
+    if (lane == 0) {
+      sh.wval[wid] = wb;
+      sh.widx[wid] = wi;
+    }
+    __syncthreads();
+    {  // CTA candidate (every warp), pushed to the cluster: warp w serves CTAs w, w + nwarps, ...
+      Real b = lane < nwarps ? sh.wval[lane] : (Real)-1;
+      int bi = lane < nwarps ? sh.widx[lane] : INT_MAX;
+      const Real b0 = b;
+      const int i0 = bi;
+      warp_argmax<C>(b, bi);
+      const unsigned msk = __ballot_sync(kFull, lane < nwarps && i0 == bi && b0 == b);
+      const int ww = msk ? __ffs(msk) - 1 : 0;
+      const C e = sh.wrow[ww][lane];
+      const Real bv = (bi != INT_MAX) ? b : (Real)-1;
+      for (int d = wid; d < cs; d += nwarps) {
+        PushShared<C>* dst = (cs > 1) ? cluster.map_shared_rank(&sh, d) : &sh;
+        dst->cand[buf][rank][lane] = e;
+        if (lane == 0) {
+          dst->cval[buf][rank] = bv;
+          dst->crow[buf][rank] = bi;
+        }
+      }
+    }
+    if (cs > 1) cluster.sync(); else __syncthreads();
+    // cluster winner (every warp reduces the cs candidates itself)
+    Real b = lane < cs ? sh.cval[buf][lane] : (Real)-1;
+    int bi = lane < cs ? sh.crow[buf][lane] : INT_MAX;
+    const Real b0 = b;
+    const int i0 = bi;
+    warp_argmax<C>(b, bi);
+    const unsigned msk = __ballot_sync(kFull, lane < cs && i0 == bi && b0 == b);
+    const int wc = msk ? __ffs(msk) - 1 : 0;
+    const int p = min(bi, m - 1);  // an unused row always exists: bi < m
+    if (tid == 0) {
+      sh.perm[t] = p;
+      if (!(b > 0) && !sh.singular) sh.singular = t + 1;
+    }
+    const C* prow = sh.cand[buf][wc];
+    const C piv = prow[t];
+    // multipliers use the reciprocal of the pivot, as LAPACK's scaling does
+    const C inv = cabs1(piv) > 0 ? cdiv(cmake<C>(1.0, 0.0), piv) : czero<C>();
+    if (prow_id == p) act = false;  // the pivot row becomes a row of U
+    if (act) {
+      const C l = cmul(vt, inv);
+#pragma unroll
+      for (int g = 0; g < kPanelNB; g += 8) {
+        if (g + 7 >= t) {  // uniform: skip groups left of the pivot column
+#pragma unroll
+          for (int c = g; c < g + 8; ++c) {
+            const C u = csub(v[c], cmul(l, prow[c]));
+            v[c] = (c > t) ? u : ((c == t) ? l : v[c]);
+          }
+        }
+      }
+    }
+  }
+  // every remote store happened before the last barrier: no CTA touches
+  // another's shared memory from here on
+  if (tid < rcount) {
+#pragma unroll
+    for (int c = 0; c < kPanelNB; ++c)
+      if (c < w) A[phys * ld + col + c] = v[c];
+  }
+  __syncthreads();
+  if (rank == 0 && wid == 0) {
+    replay_pivots(w, sh.perm, ipiv, ipiv_base, rowmap);
+    if (lane == 0 && sh.singular && info) atomicCAS(info, 0, ipiv_base + sh.singular);
+  }
+}
+
 template <typename C>
 static int panel_lu(const LaContext& ctx, int m, int w, C* A, long long ld, int col, int32_t* rowmap, int32_t* ipiv,
                     int ipiv_base) {
+  if (m <= kPushMaxCluster * kPushThreads) {
+    // 128 - 384 rows per CTA, as many CTAs (<= 16) as that takes
+    const int cs = min(kPushMaxCluster, max(1, ceil_div(m, 128)));
+    const int R = ceil_div(m, cs);
+    const int threads = ceil_div(R, 32) * 32;
+    auto kern = panel_lu_push_kernel<C>;
+    BEM_CUDA_CHECK(set_kernel_attrs_once(kern, 0, true));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ctx.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BEM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, m, w, A, ld, col, rowmap, ipiv, ipiv_base, ctx.dinfo, R));
+    count_launch();
+    return BEM200_OK;
+  }
   constexpr int kRegCap = kRegWarps * RegRows<C>::value;  // rows per CTA
   if (m <= 16 * kRegCap) {
     int cs = ceil_div(m, kRegCap);
@@ -665,16 +827,16 @@ static int panel_lu(const LaContext& ctx, int m, int w, C* A, long long ld, int 
 }
 
 // ===================================================================== TRSM leaves
-// A leaf solves with a triangle of m <= NB rows (NB = 128 for complex64, 64 for
-// complex128) held in shared memory (odd pitch).  Each warp sweeps one
+// A leaf solves with a triangle of m <= NB = 64 rows held in shared memory
+// (odd pitch); larger triangles recurse, so the work above the leaves runs as
+// GEMMs with k >= 64 (tensor cores for complex64).  Each warp sweeps one
 // right-hand vector at a time -- a column of B for left solves, a row of X for
 // right solves.  Lane l holds elements l + 32 t of the vector in registers;
 // each step of the sweep finishes one element, broadcasts it with a shuffle and
 // updates the elements still open (NB / 32 complex FMAs per lane at most).
 // Divisions by the diagonal use reciprocals computed before the sweep.  A CTA
 // owns kLeafVecs vectors, two per warp.
-template <typename C> struct LeafNB { static constexpr int value = 128; };
-template <> struct LeafNB<double2> { static constexpr int value = 64; };
+template <typename C> struct LeafNB { static constexpr int value = 64; };
 constexpr int kLeafThreads = 256;
 constexpr int kLeafVecs = 16;
 

@@ -121,8 +121,17 @@ def case_getrf(a):
         nat.call("bem200_getrf", code, a.engine, n, nat.ptr(A), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info),
                  nat.ptr(ws), wsb, nat.stream_ptr())
     go()
-    ms = _timed(go, a.reps)
-    return {"case": "getrf", "n": n, "dtype": a.dtype, "engine": a.engine, "ms": ms,
+    if a.graph:
+        # the same factorisation replayed from a CUDA graph (no host launch work)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            go()
+        g.replay()
+        ms = _timed(g.replay, a.reps)
+    else:
+        ms = _timed(go, a.reps)
+    return {"case": "getrf", "n": n, "dtype": a.dtype, "engine": a.engine, "graph": bool(a.graph), "ms": ms,
             "TFLOPs": 8.0 / 3.0 * n ** 3 / ms / 1e9, "info": int(info.item())}
 
 
@@ -139,6 +148,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--graph", action="store_true", help="getrf: replay from a CUDA graph")
     a = ap.parse_args(argv)
     import torch
     if not torch.cuda.is_available():
