@@ -144,6 +144,11 @@ size_t bem200_gemm_workspace_size(int engine, int m, int n, int k);
  * *info = first exactly-zero pivot (1-based) or 0.  All arrays are device. */
 int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
                  int32_t* info, void* ws, size_t ws_bytes, void* stream);
+/* ws of this size lets bem200_getrf run its look-ahead schedule: panels on a
+ * high-priority stream, trailing updates on a low-priority one, both forked
+ * from and joined back into `stream` (same pivots and factors).  A smaller
+ * (or NULL) ws selects the single-stream schedule. */
+size_t bem200_getrf_workspace_size(int dtype, int engine, int n);
 /* B <- A^-1 B from the getrf factors (nrhs columns, row-major B).  scratch:
  * bem200_getrs_workspace_size bytes.  *status (device int, may be NULL) is set
  * to BEM200_ERR_TIMEOUT if a bounded device-side wait of the blocked

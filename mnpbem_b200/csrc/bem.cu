@@ -27,6 +27,7 @@ struct BemState {
   C* M[kSlots];
   int32_t* map[4];   // rowmaps of LU(G1), LU(G2), LU(Delta), LU(Sigma)
   int32_t* ipiv[4];  // LAPACK swap sequences of the same factors
+  int32_t* snap[2];  // row-map snapshots of the look-ahead LU (2 n each), one per concurrent chain
   int* info;
   int* status;
 };
@@ -36,7 +37,7 @@ static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 template <typename C>
 static size_t state_bytes(int n) {
   size_t mat = align256(sizeof(C) * (size_t)n * n);
-  return kSlots * mat + 8 * align256(sizeof(int32_t) * n) + 256;
+  return kSlots * mat + 8 * align256(sizeof(int32_t) * n) + 2 * align256(sizeof(int32_t) * 2 * (size_t)n) + 256;
 }
 
 template <typename C>
@@ -52,6 +53,10 @@ static BemState<C> state_view(int n, void* ws) {
     p += align256(sizeof(int32_t) * n);
     s.ipiv[i] = reinterpret_cast<int32_t*>(p);
     p += align256(sizeof(int32_t) * n);
+  }
+  for (int i = 0; i < 2; ++i) {
+    s.snap[i] = reinterpret_cast<int32_t*>(p);
+    p += align256(sizeof(int32_t) * 2 * (size_t)n);
   }
   s.info = reinterpret_cast<int*>(p);
   s.status = s.info + 1;
@@ -147,9 +152,9 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
     }
   }
   // chain 1: LU(G1), Sigma1 = H1 G1^-1 (M5 is scratch)
-  if ((st = getrf<C>(c, n, s.M[0], n, s.map[0], s.ipiv[0], nullptr))) return st;
+  if ((st = getrf<C>(c, n, s.M[0], n, s.map[0], s.ipiv[0], s.snap[0]))) return st;
   // chain 2: LU(G2), Sigma2 = H2 G2^-1 (M4 is scratch)
-  if ((st = getrf<C>(c2, n, s.M[1], n, s.map[1], s.ipiv[1], nullptr))) return st;
+  if ((st = getrf<C>(c2, n, s.M[1], n, s.map[1], s.ipiv[1], s.snap[1]))) return st;
   if ((st = solve_right<C>(c, n, n, s.M[0], n, s.map[0], s.M[2], n, s.M[5]))) return st;
   if ((st = solve_right<C>(c2, n, n, s.M[1], n, s.map[1], s.M[3], n, fork ? s.M[4] : s.M[5]))) return st;
   if (fork) {
@@ -160,12 +165,12 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
   // Delta = Sigma1 - Sigma2, LU(Delta), Delta^-1
   delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[4]);
   BEM_LAUNCH_CHECK();
-  if ((st = getrf<C>(c, n, s.M[4], n, s.map[2], s.ipiv[2], nullptr))) return st;
+  if ((st = getrf<C>(c, n, s.M[4], n, s.map[2], s.ipiv[2], s.snap[0]))) return st;
   if ((st = inverse<C>(c, n, s.M[4], n, s.map[2], s.M[5], n))) return st;
   // Sigma, LU(Sigma)
   sigma_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(n, s.M[2], s.M[3], s.M[5], nvec, eps, k0 * k0, s.M[6]);
   BEM_LAUNCH_CHECK();
-  if ((st = getrf<C>(c, n, s.M[6], n, s.map[3], s.ipiv[3], nullptr))) return st;
+  if ((st = getrf<C>(c, n, s.M[6], n, s.map[3], s.ipiv[3], s.snap[0]))) return st;
   return BEM200_OK;
 }
 

@@ -1249,10 +1249,98 @@ static int getrf_rec(const LaContext& ctx, int n, C* A, long long ld, int32_t* r
   return getrf_rec(ctx, n, A, ld, rowmap, ipiv, col0 + w1, w - w1);
 }
 
+// Blocked right-looking LU with look-ahead (block columns of kLaNB).  Step j:
+//   panel(j)   : getrf_rec on block column j                [high-priority stream]
+//   narrow(j)  : U(j, j+1) = L(j,j)^-1 A(j, j+1) and the update of block
+//                column j+1 -- all the next panel needs     [high-priority stream]
+//   wide(j)    : the same for block columns j+2..           [low-priority stream]
+// so the wide TRSM + tensor-core GEMM of step j runs while panel(j+1) is
+// factored.  narrow(j) waits for wide(j-1), wide(j) waits for panel(j).
+// panel(j+1) permutes logical rows >= (j+1) kLaNB while wide(j) updates them,
+// so wide(j) addresses those rows through a snapshot of the row map taken
+// right after panel(j) (two snapshots alternate).  The rows themselves never
+// move, so both orders give the same matrix.
+constexpr int kLaNB = 128;
+
+struct LaStreams {
+  cudaStream_t hi = nullptr, lo = nullptr;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // fork, panel, wide, done_hi, done_lo
+  ~LaStreams() {
+    for (cudaEvent_t& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (hi) cudaStreamDestroy(hi);  // released once their queued work has finished
+    if (lo) cudaStreamDestroy(lo);
+  }
+};
+
+template <typename C>
+static int getrf_lookahead(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv,
+                           int32_t* snap) {
+  LaStreams ls;
+  int lo_pri = 0, hi_pri = 0;
+  BEM_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
+  BEM_CUDA_CHECK(cudaStreamCreateWithPriority(&ls.hi, cudaStreamNonBlocking, hi_pri));
+  BEM_CUDA_CHECK(cudaStreamCreateWithPriority(&ls.lo, cudaStreamNonBlocking, lo_pri));
+  for (cudaEvent_t& e : ls.ev) BEM_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaEvent_t ev_fork = ls.ev[0], ev_panel = ls.ev[1], ev_wide = ls.ev[2];
+  BEM_CUDA_CHECK(cudaEventRecord(ev_fork, ctx.stream));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(ls.hi, ev_fork, 0));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(ls.lo, ev_fork, 0));
+  LaContext cm = ctx, cw = ctx;
+  cm.stream = ls.hi;
+  cw.stream = ls.lo;
+  if (ctx.engine != GemmEngine::kSimt) {
+    const size_t h = (ctx.ws_bytes / 2) & ~size_t(255);
+    cm.ws_bytes = h;
+    cw.ws = reinterpret_cast<char*>(ctx.ws) + h;
+    cw.ws_bytes = h;
+  }
+  iota_kernel<<<ceil_div(n, 256), 256, 0, ls.hi>>>(n, rowmap);
+  BEM_LAUNCH_CHECK();
+  bool wide_pending = false;
+  int st;
+  for (int c0 = 0, j = 0; c0 < n; c0 += kLaNB, ++j) {
+    const int w = min(kLaNB, n - c0);
+    if ((st = getrf_rec(cm, n, A, ld, rowmap, ipiv, c0, w))) return st;
+    const int c1 = c0 + w;
+    if (c1 >= n) break;
+    const int w1 = min(kLaNB, n - c1), c2 = c1 + w1;
+    int32_t* sn = snap + (size_t)(j & 1) * n;  // sn[i] = rowmap[c1 + i] as of the end of panel(j)
+    if (c2 < n) {
+      BEM_CUDA_CHECK(cudaMemcpyAsync(sn, rowmap + c1, sizeof(int32_t) * (n - c1), cudaMemcpyDeviceToDevice, ls.hi));
+      BEM_CUDA_CHECK(cudaEventRecord(ev_panel, ls.hi));
+    }
+    // narrow(j): block column j + 1
+    if (wide_pending) BEM_CUDA_CHECK(cudaStreamWaitEvent(ls.hi, ev_wide, 0));
+    RowView<C> V{A, ld, rowmap + c0, c0};  // logical rows from c0, columns from c0
+    if ((st = trsm_llu<C>(cm, w, w1, V, V.sub(0, w)))) return st;
+    if ((st = gemm_v<C>(cm, n - c1, w1, w, neg_one<C>(), V.sub(w, 0), V.sub(0, w), one<C>(), V.sub(w, w)))) return st;
+    // wide(j): block columns j + 2 ..
+    wide_pending = false;
+    if (c2 < n) {
+      BEM_CUDA_CHECK(cudaStreamWaitEvent(ls.lo, ev_panel, 0));
+      if ((st = trsm_llu<C>(cw, w, n - c2, V, V.sub(0, c2 - c0)))) return st;
+      const RowView<C> L21{A, ld, sn, c0}, A22{A, ld, sn, c2};
+      if ((st = gemm_v<C>(cw, n - c1, n - c2, w, neg_one<C>(), L21, V.sub(0, c2 - c0), one<C>(), A22))) return st;
+      BEM_CUDA_CHECK(cudaEventRecord(ev_wide, ls.lo));
+      wide_pending = true;
+    }
+  }
+  BEM_CUDA_CHECK(cudaEventRecord(ls.ev[3], ls.hi));
+  BEM_CUDA_CHECK(cudaEventRecord(ls.ev[4], ls.lo));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(ctx.stream, ls.ev[3], 0));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(ctx.stream, ls.ev[4], 0));
+  return BEM200_OK;
+}
+
 template <typename C>
 int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv, int32_t* scratch) {
-  (void)scratch;
   BEM_REQUIRE(n > 0 && A && rowmap && ipiv && ld >= n, BEM200_ERR_ARG, "getrf: bad arguments");
+  // look-ahead needs the row-map snapshots (scratch) and, on the tensor-core
+  // engines, room for two concurrent GEMMs in the operand workspace
+  const bool ws_ok = ctx.engine == GemmEngine::kSimt ||
+                     gemm_tc_workspace(n, n, kLaNB, ctx.engine) <= ((ctx.ws_bytes / 2) & ~size_t(255));
+  if (scratch && n > 2 * kLaNB && ws_ok) return getrf_lookahead<C>(ctx, n, A, ld, rowmap, ipiv, scratch);
   iota_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(n, rowmap);
   BEM_LAUNCH_CHECK();
   return getrf_rec(ctx, n, A, ld, rowmap, ipiv, 0, n);
@@ -1393,6 +1481,15 @@ size_t bem200_gemm_workspace_size(int engine, int m, int n, int k) {
   return gemm_tc_workspace(m, n, k, engine_of(engine));
 }
 
+// ws layout for getrf: [tensor-core operand space | 2 n int32 row-map snapshots]
+static size_t getrf_snap_bytes(int n) { return ((size_t)2 * n * sizeof(int32_t) + 255) & ~size_t(255); }
+
+size_t bem200_getrf_workspace_size(int dtype, int engine, int n) {
+  (void)dtype;
+  if (n <= 0) return 0;
+  return ((gemm_tc_workspace(n, n, n, engine_of(engine)) + 255) & ~size_t(255)) + getrf_snap_bytes(n);
+}
+
 int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv, int32_t* info,
                  void* ws, size_t ws_bytes, void* stream) {
   LaContext ctx;
@@ -1401,8 +1498,14 @@ int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* row
   ctx.ws = ws;
   ctx.ws_bytes = ws_bytes;
   ctx.dinfo = info;
-  if (dtype == BEM200_C128) return getrf<double2>(ctx, n, (double2*)A, ld, rowmap, ipiv, nullptr);
-  if (dtype == BEM200_C64) return getrf<float2>(ctx, n, (float2*)A, ld, rowmap, ipiv, nullptr);
+  int32_t* snap = nullptr;
+  if (ws && n > 0 && ws_bytes >= bem200_getrf_workspace_size(dtype, engine, n)) {
+    const size_t sb = getrf_snap_bytes(n);
+    ctx.ws_bytes = (ws_bytes - sb) & ~size_t(255);
+    snap = reinterpret_cast<int32_t*>(reinterpret_cast<char*>(ws) + ctx.ws_bytes);
+  }
+  if (dtype == BEM200_C128) return getrf<double2>(ctx, n, (double2*)A, ld, rowmap, ipiv, snap);
+  if (dtype == BEM200_C64) return getrf<float2>(ctx, n, (float2*)A, ld, rowmap, ipiv, snap);
   set_error("getrf: bad dtype %d", dtype);
   return BEM200_ERR_ARG;
 }

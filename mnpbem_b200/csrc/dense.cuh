@@ -71,7 +71,9 @@ inline int gemm(const LaContext& ctx, int m, int n, int k, C alpha, const C* A, 
 }
 
 // P A = L U in place (storage rows stay put).  rowmap: n int32 (output),
-// ipiv: n int32 (output, LAPACK swap sequence, 0-based).  scratch: 4 n + 64 ints.
+// ipiv: n int32 (output, LAPACK swap sequence, 0-based).  scratch: 2 n ints
+// (row-map snapshots) selects the look-ahead schedule; NULL selects the
+// single-stream recursive one.  Both give the same pivots.
 template <typename C>
 int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv, int32_t* scratch);
 

@@ -113,7 +113,7 @@ def case_getrf(a):
     rowmap = torch.empty(n, dtype=torch.int32, device="cuda")
     ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
     info = torch.zeros(1, dtype=torch.int32, device="cuda")
-    wsb = int(nat.lib().bem200_gemm_workspace_size(a.engine, n, n, n))
+    wsb = int(nat.lib().bem200_getrf_workspace_size(code, a.engine, n))
     ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
 
     def go():

@@ -116,3 +116,59 @@ def test_gemm_skinny(cuda, dt, tol, n):
              nat.stream_ptr())
     ref = (1.5 + 0.5j) * (A.astype(np.complex128) @ B) + (-0.5 + 2j) * C
     assert np.max(np.abs(Ct.cpu().numpy() - ref)) / np.max(np.abs(ref)) < tol
+
+
+def _getrf_ws(A, engine):
+    """getrf with its full workspace: the look-ahead (two-stream) schedule."""
+    import torch
+    n = A.shape[0]
+    code = nat.C128 if A.dtype == torch.complex128 else nat.C64
+    rowmap = torch.empty(n, dtype=torch.int32, device="cuda")
+    ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    wsb = int(nat.lib().bem200_getrf_workspace_size(code, engine, n))
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    nat.call("bem200_getrf", code, engine, n, nat.ptr(A), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info),
+             nat.ptr(ws), wsb, nat.stream_ptr())
+    return rowmap, ipiv, info
+
+
+@pytest.mark.parametrize("n", [300, 1100, 1537])
+def test_getrf_lookahead_c128_matches_lapack(cuda, n):
+    A = _rand(n, n, 40 + n)
+    At = _t(A)
+    rowmap, ipiv, info = _getrf_ws(At, 0)
+    lu, piv = sla.lu_factor(A)
+    assert int(info.item()) == 0
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv)
+    got = At.cpu().numpy()[rowmap.cpu().numpy()]
+    assert np.max(np.abs(got - lu)) / np.max(np.abs(lu)) < 1e-11
+
+
+def test_getrf_lookahead_c64_tensor_cores(cuda):
+    """complex64 look-ahead LU on the bf16x3 tensor-core engine, on a
+    well-conditioned matrix (cond ~ 3, as the bf16x3 products carry ~2^-16
+    relative error): the solve error matches the single-stream schedule's."""
+    n = 1500
+    A = (_rand(n, n, 77) / np.sqrt(n) + 3 * np.eye(n)).astype(np.complex64)
+    B = _rand(n, 3, 78)
+    X = np.linalg.solve(A.astype(np.complex128), B)
+    errs = []
+    for lookahead in (True, False):
+        At = _t(A)
+        if lookahead:
+            rowmap, ipiv, info = _getrf_ws(At, 1)
+        else:
+            import torch
+            rowmap = torch.empty(n, dtype=torch.int32, device="cuda")
+            ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
+            info = torch.zeros(1, dtype=torch.int32, device="cuda")
+            wsb = int(nat.lib().bem200_gemm_workspace_size(1, n, n, n))  # too small for look-ahead
+            ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+            nat.call("bem200_getrf", nat.C64, 1, n, nat.ptr(At), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info),
+                     nat.ptr(ws), wsb, nat.stream_ptr())
+        assert int(info.item()) == 0
+        Bt = _t(B.astype(np.complex64))
+        getrs(At, rowmap, Bt)
+        errs.append(np.max(np.abs(Bt.cpu().numpy() - X)) / np.max(np.abs(X)))
+    assert errs[0] < 2e-4 and errs[0] < 3 * errs[1] + 1e-6, errs
