@@ -323,9 +323,13 @@ def roofline_gemm(dev):
         peak, src = float(mp["bf16_tflops"]), "measured bf16 burst"
     except Exception:
         pass
+    # DRAM bytes (read + write) of one launch of this GEMM from an ncu capture of the same shape
+    # (profiles/gemm_bf16x3_5768x2884x2884.md): 1.251 GB read + 0.139 GB written
+    traffic = 1.251e9 + 0.139e9
     return {"kernel": "tc::gemm_bf16x3_kernel (+ operand prep)", "bound": "tensor", "achieved": round(achieved, 2),
             "peak": peak, "peak_source": src, "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
-            "traffic": None, "shape": [m, n, k], "ms_per_launch": round(1e3 * t, 3)}
+            "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch",
+            "algorithmic_flops_per_launch": 8.0 * m * n * k, "shape": [m, n, k], "ms_per_launch": round(1e3 * t, 3)}
 
 
 def cpu_baseline(cp):

@@ -283,7 +283,7 @@ __global__ void solve_pack_kernel(int n, int p, const C* __restrict__ sig2, cons
 
 template <typename C>
 static size_t solve_scratch_bytes(int n, int p) {
-  return align256(sizeof(C) * (size_t)n * p * 20) + align256(solve_left_scratch_bytes<C>(n, 4 * p));
+  return align256(sizeof(C) * (size_t)n * p * 20) + 2 * align256(solve_left_scratch_bytes<C>(n, 4 * p));
 }
 
 // Solve for (W1 = [sig1 | h1], W2 = [sig2 | h2]) given RHS (phi, a, alpha, De)
@@ -323,8 +323,21 @@ static int bem_solve_core(const LaContext& ctx0, int n, int p, void* ws, const C
   if ((st = gemm<C>(ctx, n, 3 * p, n, one, s.M[5], n, X, 3 * p, zero, h2, 3 * p))) return st;
   solve_pack_kernel<C><<<ceil_div(4 * np, 256), 256, 0, st_>>>(n, p, rs, h2, phi, a, W1, W2);
   BEM_LAUNCH_CHECK();
+  // sig1/h1 = G1^-1 W1 and sig2/h2 = G2^-1 W2 are independent: the second runs
+  // on a stream forked from the caller's, with its own triangular-solve scratch
+  ForkJoin fj;
+  BEM_CUDA_CHECK(cudaStreamCreateWithFlags(&fj.side, cudaStreamNonBlocking));
+  BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fj.fork, cudaEventDisableTiming));
+  BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fj.join, cudaEventDisableTiming));
+  BEM_CUDA_CHECK(cudaEventRecord(fj.fork, st_));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(fj.side, fj.fork, 0));
+  LaContext c2 = ctx;
+  c2.stream = fj.side;
+  void* lscr2 = reinterpret_cast<char*>(lscr) + align256(solve_left_scratch_bytes<C>(n, 4 * p));
   if ((st = solve_left<C>(ctx, n, 4 * p, s.M[0], n, s.map[0], W1, 4 * p, lscr))) return st;
-  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[1], n, s.map[1], W2, 4 * p, lscr))) return st;
+  if ((st = solve_left<C>(c2, n, 4 * p, s.M[1], n, s.map[1], W2, 4 * p, lscr2))) return st;
+  BEM_CUDA_CHECK(cudaEventRecord(fj.join, fj.side));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(st_, fj.join, 0));
   return BEM200_OK;
 }
 
