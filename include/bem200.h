@@ -223,6 +223,40 @@ int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, c
                         const double* nvec, double k0, double tol, int maxit, void* W1, void* W2, void* scratch,
                         void* gemm_ws, size_t gemm_ws_bytes, int32_t* iters, double* relres, void* stream);
 
+/* y = M b: one application of the factors in ws (built by bem200_bem_init)
+ * as the preconditioner of the iterative solver.  b: right-hand-side layout,
+ * y: solution layout [W1 | W2], both complex128 (8 n p values).  precision 1
+ * applies the complex64 factors to b scaled to unit max-norm.  scratch:
+ * bem200_bem_solve_workspace_size(precision, n, npol) bytes.  Replaces
+ * BEMRetIter._mfun (mnpbem/bem/bem_ret_iter.py:1503-1634). */
+int bem200_bem_precond(int precision, int engine, int n, int npol, void* ws, const void* b, int eps_per_face,
+                       const double* eps1, const double* eps2, const double* nvec, double k0, void* y,
+                       void* scratch, void* gemm_ws, size_t gemm_ws_bytes, void* stream);
+
+/* x = the right-hand side b relabelled into the solution layout (phi -> sig1,
+ * a -> h1, De -> sig2, alpha -> h2): the M = I "preconditioner" of the
+ * unpreconditioned iteration, which pairs the two spaces as the reference's
+ * packed vectors do (mnpbem/bem/bem_ret_iter.py:1196-1233). */
+int bem200_bem_relabel(int n, int npol, const void* b, void* x, void* stream);
+
+/* ------------------------------------------------------------- Krylov
+ * Kernels of the restarted GMRES of the iterative solver (complex128), which
+ * replaces scipy.sparse.linalg.gmres as driven by BEMIter._iter_solve
+ * (mnpbem/bem/bem_iter.py:45-101).  A basis is m vectors of length len stored
+ * one after the other.
+ * bem200_gmres_orth: orthogonalise the vector after V_0..V_j against them
+ * (classical Gram-Schmidt, two passes; j = -1: none), normalise it, and
+ * return on the HOST
+ * h[2 i], h[2 i + 1] = <V_i, w> (i <= j) and h[2 j + 2] = ||w|| before
+ * normalisation; synchronises the stream.
+ * bem200_gmres_combine: z = sum_{i < m} y_i V_i, y complex on the HOST.
+ * bem200_zaxpy: y += a x, a = (re, im) on the HOST. */
+size_t bem200_gmres_orth_workspace_size(int j);
+int bem200_gmres_orth(int64_t len, int j, void* V, double* h_host, void* scratch, void* stream);
+int bem200_gmres_combine(int64_t len, int m, const void* V, const double* y_host, void* z, void* scratch,
+                         void* stream);
+int bem200_zaxpy(int64_t len, const double* a, const void* x, void* y, void* stream);
+
 /* dst (complex64) = src (complex128), count elements. */
 int bem200_convert_c128_c64(int64_t count, const void* src, void* dst, void* stream);
 

@@ -8,7 +8,7 @@ from .materials import EpsConst, EpsDrude, EpsTable, EpsValues
 from .planewave import CompStruct, PlaneWaveRet, SpectrumRet
 
 __all__ = ["ComParticle", "Particle", "trisphere", "EpsConst", "EpsDrude", "EpsTable", "EpsValues",
-           "CompStruct", "PlaneWaveRet", "SpectrumRet", "CompGreenRet", "BEMRet"]
+           "CompStruct", "PlaneWaveRet", "SpectrumRet", "CompGreenRet", "BEMRet", "BEMRetIter"]
 
 
 def __getattr__(name):
@@ -20,4 +20,7 @@ def __getattr__(name):
     if name == "BEMRet":
         from .bem import BEMRet
         return BEMRet
+    if name == "BEMRetIter":
+        from .bem_iter import BEMRetIter
+        return BEMRetIter
     raise AttributeError(name)

@@ -65,6 +65,13 @@ _SIGS = {
                                            ctypes.c_int, _vp, _vp, _vp, _dbl, _dbl, ctypes.c_int, _vp, _vp, _vp, _vp,
                                            _sz, _vp, _vp, _vp]),
     "bem200_convert_c128_c64": (ctypes.c_int, [_i64, _vp, _vp, _vp]),
+    "bem200_bem_precond": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                          ctypes.c_int, _vp, _vp, _vp, _dbl, _vp, _vp, _vp, _sz, _vp]),
+    "bem200_bem_relabel": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    "bem200_gmres_orth_workspace_size": (_sz, [ctypes.c_int]),
+    "bem200_gmres_orth": (ctypes.c_int, [_i64, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "bem200_gmres_combine": (ctypes.c_int, [_i64, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "bem200_zaxpy": (ctypes.c_int, [_i64, _vp, _vp, _vp, _vp]),
 }
 
 

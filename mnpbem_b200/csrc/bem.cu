@@ -578,6 +578,80 @@ int bem200_convert_c128_c64(int64_t count, const void* src, void* dst, void* str
   return BEM200_OK;
 }
 
+// The identification of the right-hand-side space with the solution space
+// used by the unpreconditioned iteration (M = I): phi -> sig1, a -> h1,
+// De -> sig2, alpha -> h2, the pairing of the reference's packed vectors
+// (pack(sig1, h1, sig2, h2) against pack(phi, a, De, alpha),
+// mnpbem/bem/bem_ret_iter.py:1196-1233, 1499).
+__global__ void relabel_kernel(int n, int p, const double2* __restrict__ b, double2* __restrict__ x) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long np = (long long)n * p;
+  if (idx >= 4 * np) return;
+  const int i = (int)(idx / (4 * p)), c = (int)(idx % (4 * p));
+  const double2* phi = b;
+  const double2* a = b + np;
+  const double2* alpha = b + 4 * np;
+  const double2* De = b + 7 * np;
+  if (c < p) {
+    x[idx] = phi[(long long)i * p + c];
+    x[4 * np + idx] = De[(long long)i * p + c];
+  } else {
+    x[idx] = a[(long long)i * 3 * p + (c - p)];
+    x[4 * np + idx] = alpha[(long long)i * 3 * p + (c - p)];
+  }
+}
+
+int bem200_bem_relabel(int n, int npol, const void* b, void* x, void* stream) {
+  BEM_REQUIRE(n > 0 && npol > 0 && b && x && b != x, BEM200_ERR_ARG, "bem_relabel: bad arguments");
+  const long long np = (long long)n * npol;
+  relabel_kernel<<<ceil_div(4 * np, 256), 256, 0, (cudaStream_t)stream>>>(n, npol, (const double2*)b, (double2*)x);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+// y = M b: one application of the factored BEM solve (the preconditioner of
+// the iterative solver).  b uses the right-hand-side layout, y the solution
+// layout [W1 | W2]; both complex128.  precision 1 runs the complex64 factors
+// (the input is scaled to unit max-norm before the cast and back after it).
+int bem200_bem_precond(int precision, int engine, int n, int npol, void* ws, const void* b, int eps_per_face,
+                       const double* eps1, const double* eps2, const double* nvec, double k0, void* y, void* scratch,
+                       void* gemm_ws, size_t gemm_ws_bytes, void* stream) {
+  BEM_REQUIRE(n > 0 && npol > 0 && ws && b && y && scratch, BEM200_ERR_ARG, "bem_precond: bad arguments");
+  LaContext ctx;
+  ctx.stream = (cudaStream_t)stream;
+  ctx.engine = engine_from(engine);
+  ctx.ws = gemm_ws;
+  ctx.ws_bytes = gemm_ws_bytes;
+  EpsArg eps = make_eps(eps_per_face, eps1, eps2);
+  const long long np = (long long)n * npol;
+  const double2* bb = (const double2*)b;
+  double2* yy = (double2*)y;
+  if (precision == 0)
+    return bem_solve_core<double2>(ctx, n, npol, ws, bb, bb + np, bb + 4 * np, bb + 7 * np, eps, nvec, k0, yy,
+                                   yy + 4 * np, (double2*)scratch);
+  char* p = reinterpret_cast<char*>(scratch);
+  float2* core = reinterpret_cast<float2*>(p);  p += align256(solve_scratch_bytes<float2>(n, npol));
+  float2* rhs32 = reinterpret_cast<float2*>(p); p += align256(sizeof(float2) * 8 * np);
+  float2* sol32 = reinterpret_cast<float2*>(p); p += align256(sizeof(float2) * 8 * np);
+  p += 2 * align256(sizeof(double2) * 8 * np) + align256(sizeof(double2) * 40 * np);
+  unsigned long long* red = reinterpret_cast<unsigned long long*>(p);
+  double bn = 0;
+  int st = absmax_host(ctx.stream, 8 * np, bb, red, &bn);
+  if (st) return st;
+  if (!(bn > 0 && bn < 1e300)) {
+    BEM_CUDA_CHECK(cudaMemsetAsync(yy, 0, sizeof(double2) * 8 * np, ctx.stream));
+    return BEM200_OK;
+  }
+  c128_to_c64_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(8 * np, bb, rhs32, 1.0 / bn);
+  BEM_LAUNCH_CHECK();
+  if ((st = bem_solve_core<float2>(ctx, n, npol, ws, rhs32, rhs32 + np, rhs32 + 4 * np, rhs32 + 7 * np, eps, nvec,
+                                   k0, sol32, sol32 + 4 * np, core)))
+    return st;
+  axpy_c64_to_c128_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(8 * np, sol32, bn, yy, false);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
 size_t bem200_bem_apply_workspace_size(int n, int npol) { return sizeof(double2) * 40 * (size_t)n * npol; }
 
 int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, const void* G2, const void* H1,

@@ -160,3 +160,41 @@ def bem_operator(G1, G2, H1, H2, eps1, eps2, nvec, enei, sig1, sig2, h1, h2):
     De = mv(H1, e1 * sig1) - mv(H2, e2 * sig2) - 1j * k * np.einsum(
         "ij,ijk->ik", nvec, mv(G1, e1h * h1) - mv(G2, e2h * h2))
     return phi, a, alpha, De
+
+
+def iter_solve(G1, G2, H1, H2, eps1, eps2, nvec, enei, phi, a, alpha, De, tol=1e-4, maxit=200, restart=None):
+    """Unpreconditioned iterative solve of the BEM system, restating
+    BEMRetIter.solve with precond=None (mnpbem/bem/bem_ret_iter.py:1636-1744):
+    scipy GMRES (BEMIter._iter_solve, mnpbem/bem/bem_iter.py:86-90, restart
+    defaulting to maxit) on x = pack(sig1, h1, sig2, h2) against
+    b = pack(phi, a, De, alpha), column-major packing (:1196-1233), with
+    the operator of ``bem_operator``.  Single polarisation.
+    Returns sig1 (n,), sig2 (n,), h1 (n,3), h2 (n,3), iterations, relres."""
+    import scipy.sparse.linalg as spl
+    n = G1.shape[0]
+
+    def pack(*arrs):
+        return np.concatenate([np.asarray(v).reshape(n, -1).ravel(order="F") for v in arrs])
+
+    def unpack_x(x):
+        s1 = x[:n]
+        h1 = x[n:4 * n].reshape(n, 3, order="F")
+        s2 = x[4 * n:5 * n]
+        h2 = x[5 * n:].reshape(n, 3, order="F")
+        return s1, h1, s2, h2
+
+    def mv(x):
+        s1, h1, s2, h2 = unpack_x(x)
+        ph, aa, al, de = bem_operator(G1, G2, H1, H2, eps1, eps2, nvec, enei, s1[:, None], s2[:, None],
+                                      h1[:, :, None], h2[:, :, None])
+        return pack(ph[:, 0], aa[:, :, 0], de[:, 0], al[:, :, 0])
+
+    b = pack(phi[:, 0], a[:, :, 0], De[:, 0], alpha[:, :, 0])
+    A = spl.LinearOperator((8 * n, 8 * n), matvec=mv, dtype=complex)
+    count = []
+    rs = restart if restart is not None else min(8 * n, maxit)
+    x, flag = spl.gmres(A, b, rtol=tol, maxiter=maxit, restart=rs, callback=lambda rk: count.append(rk),
+                        callback_type="pr_norm")
+    relres = np.linalg.norm(mv(x) - b) / np.linalg.norm(b)
+    s1, h1, s2, h2 = unpack_x(x)
+    return s1, s2, h1, h2, len(count), relres
