@@ -239,6 +239,48 @@ int bem200_bem_precond(int precision, int engine, int n, int npol, void* ws, con
  * packed vectors do (mnpbem/bem/bem_ret_iter.py:1196-1233). */
 int bem200_bem_relabel(int n, int npol, const void* b, void* x, void* stream);
 
+/* The two ends of the FP64 operator for operators whose four products are
+ * computed elsewhere (the H-matrix path): U = [s | h | e s | e h] (n x 8p)
+ * from W = [s | h] (n x 4p) with the eps of side `second` (0: eps1, 1: eps2),
+ * and r = A x (b NULL) or b - A x from GU1 = G1 U1, GU2 = G2 U2, HU1 = H1 U1,
+ * HU2 = H2 U2 (each n x 8p).  Replaces BEMRetIter._afun
+ * (mnpbem/bem/bem_ret_iter.py:1362-1501). */
+int bem200_op_prep(int n, int npol, const void* W, int eps_per_face, const double* eps1, const double* eps2,
+                   int second, void* U, void* stream);
+int bem200_op_combine(int n, int npol, const void* GU1, const void* GU2, const void* HU1, const void* HU2,
+                      const double* nvec, double k0, const void* b, void* r, void* stream);
+
+/* ------------------------------------------------------------- H-matrix
+ * complex128 H-matrices in cluster order (reference HMatrix,
+ * mnpbem/greenfun/hmatrix.py:94-541).  Blocks are (r0, m, c0, nb) int32
+ * quadruples.  Dense block b is packed at D + doff[b] (m x nb row-major);
+ * low-rank block b stores U (m x kcap[b]) at U + uoff[b] and V (nb x kcap[b])
+ * at V + voff[b], row-major, block ~ U[:, :rank] V[:, :rank]^T.
+ * bem200_hmat_permute: dst[i][j] = src[c2p[i]][c2p[j]] (n x n).
+ * bem200_hmat_gather_rows: dst[i, :] = src[idx[i], :] (n x w).
+ * bem200_hmat_aca: partially pivoted ACA of every low-rank block from the
+ *   cluster-ordered dense matrix Mc (ld n), stopping when the new rank-1 term
+ *   drops below htol times the Frobenius estimate or at rank kcap[b]
+ *   (reference HMatrix._aca_block, hmatrix.py:195-336); rank[b] on the device.
+ *   max_rows >= every m and nb, max_kcap >= every kcap.
+ * bem200_hmat_matvec: y = H x for n x w (w <= 16) row-major x, y; T holds
+ *   sum_b kcap[b] x w complex (toff[b] = prefix sum of kcap); leaf clusters
+ *   (first row, rows) with CSR lists lptr/lent of (kind 0 dense | 1 low-rank,
+ *   block) entries covering each leaf's rows (reference mtimes_vec,
+ *   hmatrix.py:450-541). */
+int bem200_hmat_permute(int n, const void* src, const int32_t* c2p, void* dst, void* stream);
+int bem200_hmat_gather_rows(int n, int w, const void* src, const int32_t* idx, void* dst, void* stream);
+int bem200_hmat_pack_dense(int nd, const int32_t* dblk, const int64_t* doff, int n, const void* Mc, void* D,
+                           void* stream);
+int bem200_hmat_aca(int nl, const int32_t* lblk, const int64_t* uoff, const int64_t* voff, const int32_t* kcap,
+                    int n, const void* Mc, double htol, void* U, void* V, int32_t* rank, int max_rows,
+                    int max_kcap, void* stream);
+int bem200_hmat_matvec(int n, int w, const void* x, int nl, const int32_t* lblk, const int64_t* voff,
+                       const int64_t* uoff, const int64_t* toff, const int32_t* kcap, const int32_t* rank,
+                       const void* U, const void* V, void* T, int nd, const int32_t* dblk, const int64_t* doff,
+                       const void* D, int nleaf, const int32_t* leaf, const int32_t* lptr, const int32_t* lent,
+                       void* y, void* stream);
+
 /* ------------------------------------------------------------- Krylov
  * Kernels of the restarted GMRES of the iterative solver (complex128), which
  * replaces scipy.sparse.linalg.gmres as driven by BEMIter._iter_solve

@@ -68,6 +68,17 @@ _SIGS = {
     "bem200_bem_precond": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                           ctypes.c_int, _vp, _vp, _vp, _dbl, _vp, _vp, _vp, _sz, _vp]),
     "bem200_bem_relabel": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    "bem200_op_prep": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp,
+                                      _vp]),
+    "bem200_op_combine": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _dbl, _vp, _vp, _vp]),
+    "bem200_hmat_gather_rows": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "bem200_hmat_permute": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "bem200_hmat_pack_dense": (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
+    "bem200_hmat_aca": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _dbl, _vp, _vp, _vp,
+                                       ctypes.c_int, ctypes.c_int, _vp]),
+    "bem200_hmat_matvec": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
+                                          _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, _vp,
+                                          _vp, _vp, _vp]),
     "bem200_gmres_orth_workspace_size": (_sz, [ctypes.c_int]),
     "bem200_gmres_orth": (ctypes.c_int, [_i64, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "bem200_gmres_combine": (ctypes.c_int, [_i64, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),

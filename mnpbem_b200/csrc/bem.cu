@@ -569,6 +569,37 @@ int bem200_bem_apply(int n, int npol, const void* G1, const void* G2, const void
                    (double2*)scratch);
 }
 
+// The two ends of the FP64 operator, for operators whose four products come
+// from elsewhere (the H-matrix path): U = [s | h | e s | e h] (n x 8p) from
+// W = [s | h] (n x 4p) with eps of side `second`, and the combination of
+// GU1 = G1 U1, GU2 = G2 U2, HU1 = H1 U1, HU2 = H2 U2 into r = A x (b NULL) or
+// r = b - A x (reference BEMRetIter._afun, mnpbem/bem/bem_ret_iter.py:1362-1501).
+int bem200_op_prep(int n, int npol, const void* W, int eps_per_face, const double* eps1, const double* eps2,
+                   int second, void* U, void* stream) {
+  BEM_REQUIRE(n > 0 && npol > 0 && W && U && eps1 && eps2, BEM200_ERR_ARG, "op_prep: bad arguments");
+  EpsArg eps = make_eps(eps_per_face, eps1, eps2);
+  const long long np = (long long)n * npol;
+  op_prep_kernel<<<ceil_div(8 * np, 256), 256, 0, (cudaStream_t)stream>>>(n, npol, (const double2*)W, eps,
+                                                                         second != 0, (double2*)U);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+int bem200_op_combine(int n, int npol, const void* GU1, const void* GU2, const void* HU1, const void* HU2,
+                      const double* nvec, double k0, const void* b, void* r, void* stream) {
+  BEM_REQUIRE(n > 0 && npol > 0 && GU1 && GU2 && HU1 && HU2 && nvec && r, BEM200_ERR_ARG,
+              "op_combine: bad arguments");
+  const long long np = (long long)n * npol;
+  const double2* bp = (const double2*)b;
+  double2* rr = (double2*)r;
+  op_combine_kernel<<<ceil_div(np, 256), 256, 0, (cudaStream_t)stream>>>(
+      n, npol, (const double2*)GU1, (const double2*)GU2, (const double2*)HU1, (const double2*)HU2, nvec, k0, bp,
+      bp ? bp + np : nullptr, bp ? bp + 4 * np : nullptr, bp ? bp + 7 * np : nullptr, rr, rr + np, rr + 4 * np,
+      rr + 7 * np);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
 int bem200_convert_c128_c64(int64_t count, const void* src, void* dst, void* stream) {
   BEM_REQUIRE(count >= 0 && (count == 0 || (src && dst)), BEM200_ERR_ARG, "convert: bad arguments");
   if (count == 0) return BEM200_OK;

@@ -21,8 +21,10 @@ input/output vectors that pin the oracle and the geometry module:
 * ``dimer_cfg1.npz``    : ext / sca of the 5768-face dimer (2 x trisphere(1444, 40),
                           +-21 nm on x, water, Drude gold) at 650 nm, plus
                           checksums of sig (slow: ~1 min).
+* ``hmat_trees.npz``    : reference cluster trees, admissibility block lists and
+                          ACA ranks / errors for the sphere and the small dimer.
 
-Usage:  python tests/golden/make_golden.py [--skip-cfg1]
+Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only]
 """
 import os
 import sys
@@ -159,7 +161,45 @@ def dimer_cfg1():
          sig2_head=sig.sig2[:64], ctor_s=t1 - t0, solve_s=t2 - t1)
 
 
+def hmat_trees():
+    """Cluster trees, block partitions and ACA ranks of the reference H-matrix
+    (mnpbem/greenfun/clustertree.py, hmatrix.py) for the sphere (cleaf 32,
+    eta 1) and the small dimer (cleaf 64, eta 2.5), with the wavenumber-aware
+    admissibility at 600 nm and ACA (htol 1e-6, kmax 100) of the dense G1 = G11 - G21
+    (vacuum sphere: G11 alone) at 600 nm."""
+    from mnpbem.greenfun.clustertree import ClusterTree
+    from mnpbem.greenfun.hmatrix import HMatrix, make_kaware_fadmiss
+    out = {}
+    enei = 600.0
+    cases = (("s", ComParticle([EpsConst(1.0), EpsDrude(*DRUDE_AU)], [trisphere(144, 20)], [[2, 1]], 1,
+                               interp="curv"), 32, 1.0),
+             ("d", _dimer(144, 10.0, 1.0), 64, 2.5))
+    for tag, p, cleaf, eta in cases:
+        ip = None
+        if len(p.p) > 1:
+            ip = np.concatenate([np.full(q.n, i) for i, q in enumerate(p.p)])
+        tree = ClusterTree(p.pos, cleaf=cleaf, ipart_arr=ip)
+        out[tag + "_son"], out[tag + "_cind"], out[tag + "_ind"] = tree.son, tree.cind, tree.ind
+        out[tag + "_mid"], out[tag + "_rad"], out[tag + "_ipart"] = tree.mid, tree.rad, tree.ipart
+        h = HMatrix(tree=tree, htol=1e-6, kmax=100, fadmiss=make_kaware_fadmiss(2 * np.pi / enei, eta0=eta))
+        out[tag + "_row1"], out[tag + "_col1"] = h.row1, h.col1
+        out[tag + "_row2"], out[tag + "_col2"] = h.row2, h.col2
+        bem = BEMRet(p)
+        G = bem.g.eval(0, 0, "G", enei)
+        G21 = bem.g.eval(1, 0, "G", enei)
+        if not np.isscalar(G21):
+            G = G - G21
+        h.aca(lambda r, c: G[r, c])
+        out[tag + "_ranks"] = np.array([u.shape[1] for u in h.lhs])
+        full = h.full(xp=np) if "xp" in h.full.__code__.co_varnames else h.full()
+        out[tag + "_aca_err"] = np.linalg.norm(full - G) / np.linalg.norm(G)
+    save("hmat_trees.npz", **out)
+
+
 if __name__ == "__main__":
+    hmat_trees()
+    if "--hmat-only" in sys.argv:
+        sys.exit(0)
     geom()
     refined_cfg0()
     matrices_s60()
