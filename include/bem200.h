@@ -264,10 +264,9 @@ int bem200_op_combine(int n, int npol, const void* GU1, const void* GU2, const v
  *   (reference HMatrix._aca_block, hmatrix.py:195-336); rank[b] on the device.
  *   max_rows >= every m and nb, max_kcap >= every kcap.
  * bem200_hmat_matvec: y = H x for n x w (w <= 16) row-major x, y; T holds
- *   sum_b kcap[b] x w complex (toff[b] = prefix sum of kcap); leaf clusters
- *   (first row, rows) with CSR lists lptr/lent of (kind 0 dense | 1 low-rank,
- *   block) entries covering each leaf's rows (reference mtimes_vec,
- *   hmatrix.py:450-541). */
+ *   sum_b kcap[b] x w complex (toff[b] = prefix sum of kcap).  Block rows are
+ *   added into y with atomics, so the summation order (and the last bits of
+ *   y) can vary between calls (reference mtimes_vec, hmatrix.py:450-541). */
 int bem200_hmat_permute(int n, const void* src, const int32_t* c2p, void* dst, void* stream);
 int bem200_hmat_gather_rows(int n, int w, const void* src, const int32_t* idx, void* dst, void* stream);
 int bem200_hmat_pack_dense(int nd, const int32_t* dblk, const int64_t* doff, int n, const void* Mc, void* D,
@@ -278,8 +277,7 @@ int bem200_hmat_aca(int nl, const int32_t* lblk, const int64_t* uoff, const int6
 int bem200_hmat_matvec(int n, int w, const void* x, int nl, const int32_t* lblk, const int64_t* voff,
                        const int64_t* uoff, const int64_t* toff, const int32_t* kcap, const int32_t* rank,
                        const void* U, const void* V, void* T, int nd, const int32_t* dblk, const int64_t* doff,
-                       const void* D, int nleaf, const int32_t* leaf, const int32_t* lptr, const int32_t* lent,
-                       void* y, void* stream);
+                       const void* D, void* y, void* stream);
 
 /* ------------------------------------------------------------- Krylov
  * Kernels of the restarted GMRES of the iterative solver (complex128), which

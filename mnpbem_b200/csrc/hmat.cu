@@ -232,56 +232,87 @@ __global__ void __launch_bounds__(kHThreads) hmat_vt_kernel(const int32_t* __res
   }
 }
 
-// Phase B: one CTA per leaf row cluster, one warp per row; lanes split the
-// inner dimension of every dense / low-rank row that covers it.
+// Phase B: one CTA per block (dense blocks first, then low-rank ones):
+// y[rows] += M_b S_b, with M_b the packed dense block (S_b = the x rows of its
+// columns) or the U factor (S_b = T_b).  S_b is staged in shared memory in
+// chunks of kSChunk rows with an odd pitch; 8 lanes share a matrix row (so a
+// warp covers 4 rows, each read coalesced 128 B at a time), reduce over
+// their 8 partial sums with 3 shuffle levels, and add the row into y with
+// FP64 atomics (y is zeroed first).
+constexpr int kSChunk = 128;
+
 template <int W>
-__global__ void __launch_bounds__(kHThreads) hmat_rows_kernel(
-    int w, const double2* __restrict__ x, const int32_t* __restrict__ lblk, const int64_t* __restrict__ uoff,
+__global__ void __launch_bounds__(kHThreads) hmat_block_kernel(
+    int nd, int w, const double2* __restrict__ x, const int32_t* __restrict__ lblk, const int64_t* __restrict__ uoff,
     const int64_t* __restrict__ toff, const int32_t* __restrict__ kcap_arr, const int32_t* __restrict__ rank_arr,
     const double2* __restrict__ Ug, const double2* __restrict__ T, const int32_t* __restrict__ dblk,
-    const int64_t* __restrict__ doff, const double2* __restrict__ D, const int32_t* __restrict__ leaf,
-    const int32_t* __restrict__ lptr, const int32_t* __restrict__ lent, double2* __restrict__ y) {
-  const int L = blockIdx.x;
-  const int l0 = leaf[2 * L], lm = leaf[2 * L + 1];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int e0 = lptr[L], e1 = lptr[L + 1];
-  for (int r = l0 + wid; r < l0 + lm; r += kHThreads / 32) {
+    const int64_t* __restrict__ doff, const double2* __restrict__ D, double2* __restrict__ y) {
+  __shared__ double2 Ss[kSChunk][W + 1];
+  const int b = blockIdx.x;
+  int r0, m, K, ldm;
+  const double2* M;
+  const double2* S;
+  if (b < nd) {
+    r0 = dblk[4 * b];
+    m = dblk[4 * b + 1];
+    K = dblk[4 * b + 3];
+    ldm = K;
+    M = D + doff[b];
+    S = x + (long long)dblk[4 * b + 2] * w;
+  } else {
+    const int l = b - nd;
+    r0 = lblk[4 * l];
+    m = lblk[4 * l + 1];
+    K = rank_arr[l];
+    ldm = kcap_arr[l];
+    M = Ug + uoff[l];
+    S = T + toff[l] * w;
+  }
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int js = lane & 7, rs = lane >> 3;  // 8 lanes per row, 4 rows per warp
+  for (int rbase = 0; rbase < m; rbase += 4 * (kHThreads / 32)) {
+    const int rl = rbase + 4 * wid + rs;
+    const bool rok = rl < m;
     double2 acc[W];
 #pragma unroll
     for (int q = 0; q < W; ++q) acc[q] = make_double2(0, 0);
-    for (int e = e0; e < e1; ++e) {
-      const int kind = lent[2 * e], b = lent[2 * e + 1];
-      const double2* row;
-      const double2* small;
-      int K;
-      if (kind == 0) {
-        const int r0 = dblk[4 * b], c0 = dblk[4 * b + 2], nb = dblk[4 * b + 3];
-        row = D + doff[b] + (long long)(r - r0) * nb;
-        small = x + (long long)c0 * w;
-        K = nb;
-      } else {
-        const int r0 = lblk[4 * b];
-        const int kc = kcap_arr[b];
-        row = Ug + uoff[b] + (long long)(r - r0) * kc;
-        small = T + toff[b] * w;
-        K = rank_arr[b];
+    for (int k0 = 0; k0 < K; k0 += kSChunk) {
+      const int kn = min(kSChunk, K - k0);
+      __syncthreads();
+      for (int e = tid; e < kn * w; e += kHThreads) {
+        const int j = e / w, q = e % w;
+        Ss[j][q] = S[(long long)(k0 + j) * w + q];
       }
-      for (int j = lane; j < K; j += 32) {
-        const double2 a = row[j];
+      __syncthreads();
+      if (rok) {
+        const double2* mrow = M + (long long)rl * ldm + k0;
+#pragma unroll 4
+        for (int j = js; j < kn; j += 8) {
+          const double2 a = mrow[j];
 #pragma unroll
-        for (int q = 0; q < W; ++q)
-          if (q < w) acc[q] = cadd(acc[q], cmul(a, small[(long long)j * w + q]));
+          for (int q = 0; q < W; ++q)
+            if (q < w) acc[q] = cadd(acc[q], cmul(a, Ss[j][q]));
+        }
       }
     }
 #pragma unroll
     for (int q = 0; q < W; ++q) {
       double2 v = acc[q];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
+      for (int o = 4; o > 0; o >>= 1) {
         v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
         v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
       }
-      if (lane == 0 && q < w) y[(long long)r * w + q] = v;
+      acc[q] = v;
+    }
+    if (rok) {
+#pragma unroll
+      for (int q = 0; q < W; ++q)
+        if (q < w && q % 8 == js) {
+          double* out = reinterpret_cast<double*>(y + (long long)(r0 + rl) * w + q);
+          atomicAdd(out, acc[q].x);
+          atomicAdd(out + 1, acc[q].y);
+        }
     }
   }
 }
@@ -337,24 +368,25 @@ int bem200_hmat_aca(int nl, const int32_t* lblk, const int64_t* uoff, const int6
 int bem200_hmat_matvec(int n, int w, const void* x, int nl, const int32_t* lblk, const int64_t* voff,
                        const int64_t* uoff, const int64_t* toff, const int32_t* kcap, const int32_t* rank,
                        const void* U, const void* V, void* T, int nd, const int32_t* dblk, const int64_t* doff,
-                       const void* D, int nleaf, const int32_t* leaf, const int32_t* lptr, const int32_t* lent,
-                       void* y, void* stream) {
-  BEM_REQUIRE(n > 0 && w > 0 && w <= 16 && x && y && nleaf > 0 && leaf && lptr && lent, BEM200_ERR_ARG,
+                       const void* D, void* y, void* stream) {
+  BEM_REQUIRE(n > 0 && w > 0 && w <= 16 && x && y && nl >= 0 && nd >= 0, BEM200_ERR_ARG,
               "hmat_matvec: bad arguments (w <= 16 columns)");
   cudaStream_t s = (cudaStream_t)stream;
+  BEM_CUDA_CHECK(cudaMemsetAsync(y, 0, sizeof(double2) * (size_t)n * w, s));
   if (nl > 0) {
     hmat_vt_kernel<<<nl, kHThreads, 0, s>>>(lblk, voff, toff, kcap, rank, w, (const double2*)x, (const double2*)V,
                                            (double2*)T);
     BEM_LAUNCH_CHECK();
   }
+  if (nd + nl == 0) return BEM200_OK;
   if (w <= 8)
-    hmat_rows_kernel<8><<<nleaf, kHThreads, 0, s>>>(w, (const double2*)x, lblk, uoff, toff, kcap, rank,
-                                                    (const double2*)U, (const double2*)T, dblk, doff,
-                                                    (const double2*)D, leaf, lptr, lent, (double2*)y);
+    hmat_block_kernel<8><<<nd + nl, kHThreads, 0, s>>>(nd, w, (const double2*)x, lblk, uoff, toff, kcap, rank,
+                                                       (const double2*)U, (const double2*)T, dblk, doff,
+                                                       (const double2*)D, (double2*)y);
   else
-    hmat_rows_kernel<16><<<nleaf, kHThreads, 0, s>>>(w, (const double2*)x, lblk, uoff, toff, kcap, rank,
-                                                     (const double2*)U, (const double2*)T, dblk, doff,
-                                                     (const double2*)D, leaf, lptr, lent, (double2*)y);
+    hmat_block_kernel<16><<<nd + nl, kHThreads, 0, s>>>(nd, w, (const double2*)x, lblk, uoff, toff, kcap, rank,
+                                                        (const double2*)U, (const double2*)T, dblk, doff,
+                                                        (const double2*)D, (double2*)y);
   BEM_LAUNCH_CHECK();
   return BEM200_OK;
 }

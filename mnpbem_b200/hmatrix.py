@@ -18,8 +18,8 @@ Device side (libbem200, csrc/hmat.cu):
   (hmatrix.py:195-336, tolerance ``htol``, rank <= ``kmax``); dense leaves are
   packed;
 * the product H x runs in two kernels: T_b = V_b^T x for every low-rank block,
-  then one CTA per leaf row cluster sums its dense and low-rank rows
-  (reference HMatrix.mtimes_vec, hmatrix.py:450-541).
+  then one CTA per block adds its rows, M_b times the block's x (or T) slice,
+  into y (reference HMatrix.mtimes_vec, hmatrix.py:450-541).
 
 The reference compresses each region-pair Green matrix (G11, G21, ...) and
 forms G1 = G11 - G21 by H-matrix addition with QR/SVD recompression
@@ -222,25 +222,6 @@ class HMatrixGPU:
         self.rank = torch.zeros(max(len(lb), 1), dtype=torch.int32, device=dev)
         self.c2p = t(tree.ind[:, 0].astype(np.int32))
         self.p2c = t(tree.ind[:, 1].astype(np.int32))
-        # row lists per leaf cluster: (kind, block) pairs covering its rows
-        leaves = [i for i in range(len(tree.son)) if tree.is_leaf(i)]
-        leaves.sort(key=lambda i: tree.cind[i, 0])
-        ent = [[] for _ in leaves]
-        starts = np.array([tree.cind[i, 0] for i in leaves])
-        ends = np.array([tree.cind[i, 1] for i in leaves])
-        for b, (r0, m, _, _) in enumerate(db):
-            for li in np.nonzero((starts >= r0) & (ends <= r0 + m - 1))[0]:
-                ent[li].append((0, b))
-        for b, (r0, m, _, _) in enumerate(lb):
-            for li in np.nonzero((starts >= r0) & (ends <= r0 + m - 1))[0]:
-                ent[li].append((1, b))
-        lptr = np.zeros(len(leaves) + 1, dtype=np.int32)
-        lptr[1:] = np.cumsum([len(e) for e in ent])
-        flat = np.array([x for e in ent for x in e], dtype=np.int32).reshape(-1, 2)
-        self.nleaf = len(leaves)
-        self.leaf = t(np.stack([starts, ends - starts + 1], axis=1).astype(np.int32).reshape(-1))
-        self.lptr = t(lptr)
-        self.lent = t(flat.reshape(-1) if len(flat) else np.zeros(2, np.int32))
         self.ranks = None
 
     def compress(self, M, scratch=None):
@@ -278,8 +259,7 @@ class HMatrixGPU:
         nat.call("bem200_hmat_matvec", self.n, w, nat.ptr(x), self.nlow, nat.ptr(self.lblk), nat.ptr(self.voff),
                  nat.ptr(self.uoff), nat.ptr(self.toff), nat.ptr(self.kcap), nat.ptr(self.rank), nat.ptr(self.U),
                  nat.ptr(self.V), nat.ptr(tbuf), self.ndense, nat.ptr(self.dblk), nat.ptr(self.doff),
-                 nat.ptr(self.D), self.nleaf, nat.ptr(self.leaf), nat.ptr(self.lptr), nat.ptr(self.lent), nat.ptr(y),
-                 nat.stream_ptr())
+                 nat.ptr(self.D), nat.ptr(y), nat.stream_ptr())
 
 
 def particle_index(p):

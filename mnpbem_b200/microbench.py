@@ -4,6 +4,8 @@
     python -m mnpbem_b200.microbench green [--faces 1444] [--dtype c128|c64] [--reps 3]
     python -m mnpbem_b200.microbench gemm  [--m 5768 --n 2884 --k 2884] [--engine 1] [--reps 3]
     python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1]
+    python -m mnpbem_b200.microbench hmat  [--faces 1444] [--cleaf 200] [--htol 1e-6] [--reps 3]
+    python -m mnpbem_b200.microbench iter  [--faces 1444] [--hmatrix] [--noprecond] [--tol 1e-10]
 
 ``step`` runs whole per-wavelength solves (assembly + init + solve) of the
 sphere dimer (two trisphere(faces) spheres, 2 nm gap, water, Drude gold,
@@ -135,9 +137,63 @@ def case_getrf(a):
             "TFLOPs": 8.0 / 3.0 * n ** 3 / ms / 1e9, "info": int(info.item())}
 
 
+def case_hmat(a):
+    """H-matrix of the dimer's G1: build (dense assembly + ACA of the four
+    BEM matrices), compression and the matvec with 8 right-hand columns."""
+    import torch
+    from .greenfun import CompGreenRet
+    from .hmatrix import BEMHMatrices
+    cp = dimer(a.faces)
+    g = CompGreenRet(cp, cp)
+    hb = BEMHMatrices(cp, g, htol=a.htol, kmax=100, cleaf=a.cleaf, eta=2.5)
+    hb.build(650.0)
+    ms_build = _timed(lambda: hb.build(650.0), 1)
+    h = hb.H[0]
+    n, w = cp.n, 8
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(n, w, dtype=torch.complex128, device="cuda", generator=gen)
+    y = torch.empty_like(x)
+    h.matvec(x, y, w)
+    ms_mv = _timed(lambda: h.matvec(x, y, w), a.reps)
+    stored = int(h._doff_h[-1]) + int(np.sum(h.ranks.astype(np.int64) * (h._lb[:, 1] + h._lb[:, 3])))
+    nbytes = 16 * stored
+    return {"case": "hmat", "faces": n, "cleaf": a.cleaf, "htol": a.htol, "ms_build_4_matrices": ms_build,
+            "compression": hb.compression(), "dense_blocks": h.ndense, "lowrank_blocks": h.nlow,
+            "max_rank": int(h.ranks.max()) if h.nlow else 0, "ms_matvec_w8": ms_mv,
+            "matvec_factor_GBps": nbytes / ms_mv / 1e6, "dense_matvec_bytes": 16 * n * n}
+
+
+def case_iter(a):
+    """BEMRetIter solves of the dimer (dense or H-matrix operator, complex64
+    factors as preconditioner): init (+ compression) and GMRES per wavelength."""
+    import torch
+    from . import PlaneWaveRet
+    from .bem_iter import BEMRetIter
+    cp = dimer(a.faces)
+    exc = PlaneWaveRet(np.array([[1.0, 0, 0]]), np.array([[0, 0, 1.0]]))
+    bem = BEMRetIter(cp, hmatrix=a.hmatrix, cleaf=a.cleaf, htol=a.htol, tol=a.tol,
+                     precond=None if a.noprecond else "hmat")
+    out = {"case": "iter", "faces": cp.n, "hmatrix": a.hmatrix, "tol": a.tol, "precond": not a.noprecond}
+    for rep in range(2):
+        lam = 650.0 + rep
+        e0, e1, e2 = _events() + (torch.cuda.Event(enable_timing=True),)
+        torch.cuda.synchronize()
+        e0.record()
+        bem.init(lam)
+        e1.record()
+        b, npol = bem._bem.rhs(exc.potential(cp, lam))
+        bt = torch.as_tensor(b, dtype=torch.complex128, device="cuda")
+        bem.solve_device(bt, npol)
+        e2.record()
+        torch.cuda.synchronize()
+        out["ms_init"], out["ms_solve"] = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    out["iters"], out["relres"] = bem.last.iter, bem.last.relres
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["step", "green", "gemm", "getrf"])
+    ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter"])
     ap.add_argument("--faces", type=int, default=1444)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--engine", type=int, default=1)
@@ -149,13 +205,19 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--graph", action="store_true", help="getrf: replay from a CUDA graph")
+    ap.add_argument("--cleaf", type=int, default=200)
+    ap.add_argument("--htol", type=float, default=1e-6)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--hmatrix", action="store_true")
+    ap.add_argument("--noprecond", action="store_true")
     a = ap.parse_args(argv)
     import torch
     if not torch.cuda.is_available():
         raise RuntimeError("microbench needs a CUDA device")
     if a.case == "step":
         a.engine = {0: "simt", 1: "bf16x3", 2: "tf32"}[a.engine]
-    out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf}[a.case](a)
+    out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf, "hmat": case_hmat,
+           "iter": case_iter}[a.case](a)
     print(json.dumps(out), flush=True)
 
 
