@@ -27,7 +27,7 @@ struct BemState {
   C* M[kSlots];
   int32_t* map[4];   // rowmaps of LU(G1), LU(G2), LU(Delta), LU(Sigma)
   int32_t* ipiv[4];  // LAPACK swap sequences of the same factors
-  int32_t* snap[2];  // row-map snapshots of the look-ahead LU (2 n each), one per concurrent chain
+  int32_t* snap[2];  // look-ahead LU scratch (2 n row-map snapshots + grid-panel slots), one per chain
   int* info;
   int* status;
 };
@@ -37,7 +37,8 @@ static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 template <typename C>
 static size_t state_bytes(int n) {
   size_t mat = align256(sizeof(C) * (size_t)n * n);
-  return kSlots * mat + 8 * align256(sizeof(int32_t) * n) + 2 * align256(sizeof(int32_t) * 2 * (size_t)n) + 256;
+  return kSlots * mat + 8 * align256(sizeof(int32_t) * n) +
+         2 * (align256(sizeof(int32_t) * 2 * (size_t)n) + kPanelGridScratch) + 256;
 }
 
 template <typename C>
@@ -54,9 +55,9 @@ static BemState<C> state_view(int n, void* ws) {
     s.ipiv[i] = reinterpret_cast<int32_t*>(p);
     p += align256(sizeof(int32_t) * n);
   }
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < 2; ++i) {  // snapshots, then the grid-panel candidate slots
     s.snap[i] = reinterpret_cast<int32_t*>(p);
-    p += align256(sizeof(int32_t) * 2 * (size_t)n);
+    p += align256(sizeof(int32_t) * 2 * (size_t)n) + kPanelGridScratch;
   }
   s.info = reinterpret_cast<int*>(p);
   s.status = s.info + 1;

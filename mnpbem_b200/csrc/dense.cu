@@ -751,6 +751,148 @@ __global__ void __launch_bounds__(kPushThreads, 1) panel_lu_push_kernel(int m, i
   }
 }
 
+// ----------------------------------------------------------------------------
+// Grid-wide panel for tall panels (more rows than a 16-CTA cluster holds):
+// one row per thread as in the push panel, CTAs spread over the whole GPU and
+// launched cooperatively (all resident), one grid barrier per column.  Each
+// CTA writes its best candidate (value, panel row, 32 elements) to a double
+// buffered global slot before the barrier; after it, warp 0 of every CTA
+// reduces the gridDim.x candidates (L2 reads, bypassing L1 so that a slot
+// rewritten two columns later is never read stale) and stages the pivot row
+// in shared memory.
+constexpr int kGridMaxCta = 160;
+
+template <typename C>
+struct GridCand {
+  C row[kPanelNB];
+  R_t<C> val;
+  int idx;
+};
+
+template <typename C>
+__global__ void __launch_bounds__(kPushThreads, 1) panel_lu_grid_kernel(int m, int w, C* __restrict__ A, long long ld,
+                                                                        int col, int32_t* __restrict__ rowmap,
+                                                                        int32_t* __restrict__ ipiv, int ipiv_base,
+                                                                        int* __restrict__ info, int R,
+                                                                        GridCand<C>* __restrict__ cand) {
+  using Real = R_t<C>;
+  cg::grid_group grid = cg::this_grid();
+  const int G = (int)gridDim.x, rank = (int)blockIdx.x;
+  __shared__ C wrow[kPushWarps][kPanelNB];
+  __shared__ Real wval[kPushWarps];
+  __shared__ int widx[kPushWarps];
+  __shared__ C prow[kPanelNB];
+  __shared__ int perm[kPanelNB];
+  __shared__ int sp, singular;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int r0 = rank * R;
+  const int rcount = max(0, min(R, m - r0));
+  const int prow_id = r0 + tid;
+  bool act = tid < rcount;
+  const long long phys = act ? (long long)rowmap[prow_id] : 0;
+  C v[kPanelNB];
+#pragma unroll
+  for (int c = 0; c < kPanelNB; ++c) v[c] = (act && c < w) ? A[phys * ld + col + c] : czero<C>();
+  if (tid == 0) singular = 0;
+  const unsigned kFull = 0xffffffffu;
+#pragma unroll 1
+  for (int t = 0; t < w; ++t) {
+    GridCand<C>* slots = cand + (size_t)(t & 1) * G;
+    C vt = v[0];
+#pragma unroll
+    for (int c = 1; c < kPanelNB; ++c)
+      if (c == t) vt = v[c];
+    Real wb = act ? pmag(vt) : (Real)-1;
+    int wi = act ? prow_id : INT_MAX;
+    warp_argmax<C>(wb, wi);
+    if (act && wi == prow_id) {
+#pragma unroll
+      for (int c = 0; c < kPanelNB; ++c) wrow[wid][c] = v[c];
+    }
+    if (lane == 0) {
+      wval[wid] = wb;
+      widx[wid] = wi;
+    }
+    __syncthreads();
+    if (wid == 0) {
+      Real b = lane < nwarps ? wval[lane] : (Real)-1;
+      int bi = lane < nwarps ? widx[lane] : INT_MAX;
+      const Real b0 = b;
+      const int i0 = bi;
+      warp_argmax<C>(b, bi);
+      const unsigned msk = __ballot_sync(kFull, lane < nwarps && i0 == bi && b0 == b);
+      const int ww = msk ? __ffs(msk) - 1 : 0;
+      slots[rank].row[lane] = wrow[ww][lane];
+      if (lane == 0) {
+        slots[rank].val = (bi != INT_MAX) ? b : (Real)-1;
+        slots[rank].idx = bi;
+      }
+      __threadfence();
+    }
+    grid.sync();
+    if (wid == 0) {
+      Real b = -1;
+      int bi = INT_MAX;
+      for (int g = lane; g < G; g += 32) {
+        const Real gv = __ldcg(&slots[g].val);
+        const int gi = __ldcg(&slots[g].idx);
+        if (gv > b || (gv == b && gi < bi)) {
+          b = gv;
+          bi = gi;
+        }
+      }
+      warp_argmax<C>(b, bi);
+      // the CTA that published the winning row
+      int own = INT_MAX;
+      for (int g = lane; g < G; g += 32)
+        if (__ldcg(&slots[g].idx) == bi) own = min(own, g);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) own = min(own, __shfl_xor_sync(kFull, own, o));
+      const int wc = own < G ? own : 0;
+      const C* src = &slots[wc].row[0];
+      C e;
+      e.x = __ldcg(&src[lane].x);
+      e.y = __ldcg(&src[lane].y);
+      prow[lane] = e;
+      if (lane == 0) {
+        const int p = min(bi, m - 1);  // an unused row always exists: bi < m
+        sp = p;
+        perm[t] = p;
+        if (!(b > 0) && !singular) singular = t + 1;
+      }
+    }
+    __syncthreads();
+    const int p = sp;
+    const C piv = prow[t];
+    const C inv = cabs1(piv) > 0 ? cdiv(cmake<C>(1.0, 0.0), piv) : czero<C>();
+    if (prow_id == p) act = false;
+    if (act) {
+      const C l = cmul(vt, inv);
+#pragma unroll
+      for (int g8 = 0; g8 < kPanelNB; g8 += 8) {
+        if (g8 + 7 >= t) {
+#pragma unroll
+          for (int c = g8; c < g8 + 8; ++c) {
+            const C u = csub(v[c], cmul(l, prow[c]));
+            v[c] = (c > t) ? u : ((c == t) ? l : v[c]);
+          }
+        }
+      }
+    }
+    __syncthreads();  // prow / sp are rewritten by warp 0 in the next column
+  }
+  if (tid < rcount) {
+#pragma unroll
+    for (int c = 0; c < kPanelNB; ++c)
+      if (c < w) A[phys * ld + col + c] = v[c];
+  }
+  if (rank == 0 && wid == 0) {
+    replay_pivots(w, perm, ipiv, ipiv_base, rowmap);
+    if (lane == 0 && singular && info) atomicCAS(info, 0, ipiv_base + singular);
+  }
+}
+
 template <typename C>
 static int panel_lu(const LaContext& ctx, int m, int w, C* A, long long ld, int col, int32_t* rowmap, int32_t* ipiv,
                     int ipiv_base) {
@@ -774,6 +916,28 @@ static int panel_lu(const LaContext& ctx, int m, int w, C* A, long long ld, int 
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     BEM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, m, w, A, ld, col, rowmap, ipiv, ipiv_base, ctx.dinfo, R));
+    count_launch();
+    return BEM200_OK;
+  }
+  if (ctx.panel_ws) {
+    // taller than one cluster holds: one row per thread over the whole GPU
+    static_assert(2 * kGridMaxCta * sizeof(GridCand<double2>) <= kPanelGridScratch, "panel scratch too small");
+    const int G = ceil_div(m, kPushThreads);
+    const int R = ceil_div(m, G);
+    const int threads = ceil_div(R, 32) * 32;
+    auto kern = panel_lu_grid_kernel<C>;
+    int dev = 0, nsm = 0, per_sm = 0;
+    BEM_CUDA_CHECK(cudaGetDevice(&dev));
+    BEM_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    BEM_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0));
+    BEM_REQUIRE(G <= kGridMaxCta && G <= per_sm * nsm, BEM200_ERR_UNSUPPORTED,
+                "panel_lu: panel of %d rows needs %d co-resident CTAs (device holds %d)", m, G, per_sm * nsm);
+    GridCand<C>* cand = reinterpret_cast<GridCand<C>*>(ctx.panel_ws);
+    int ipb = ipiv_base;
+    int* info = ctx.dinfo;
+    void* args[] = {(void*)&m, (void*)&w, (void*)&A, (void*)&ld, (void*)&col, (void*)&rowmap, (void*)&ipiv,
+                    (void*)&ipb, (void*)&info, (void*)&R, (void*)&cand};
+    BEM_CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)kern, dim3(G), dim3(threads), args, 0, ctx.stream));
     count_launch();
     return BEM200_OK;
   }
@@ -1289,6 +1453,7 @@ static int getrf_lookahead(const LaContext& ctx, int n, C* A, long long ld, int3
   LaContext cm = ctx, cw = ctx;
   cm.stream = ls.hi;
   cw.stream = ls.lo;
+  cm.panel_ws = reinterpret_cast<char*>(snap) + (((size_t)2 * n * sizeof(int32_t) + 255) & ~size_t(255));
   if (ctx.engine != GemmEngine::kSimt) {
     const size_t h = (ctx.ws_bytes / 2) & ~size_t(255);
     cm.ws_bytes = h;
@@ -1482,7 +1647,9 @@ size_t bem200_gemm_workspace_size(int engine, int m, int n, int k) {
 }
 
 // ws layout for getrf: [tensor-core operand space | 2 n int32 row-map snapshots]
-static size_t getrf_snap_bytes(int n) { return ((size_t)2 * n * sizeof(int32_t) + 255) & ~size_t(255); }
+static size_t getrf_snap_bytes(int n) {
+  return (((size_t)2 * n * sizeof(int32_t) + 255) & ~size_t(255)) + kPanelGridScratch;
+}
 
 size_t bem200_getrf_workspace_size(int dtype, int engine, int n) {
   (void)dtype;

@@ -58,7 +58,11 @@ struct LaContext {
   size_t ws_bytes = 0;
   int* dinfo = nullptr;     // device int: first exactly-zero pivot (1-based) or 0
   int* dstatus = nullptr;   // device int: set to a non-zero code if a bounded wait gave up
+  void* panel_ws = nullptr; // candidate slots of the grid-wide panel (panels of more rows than a cluster holds)
 };
+
+// bytes of the grid-wide panel's candidate slots (2 x up to 160 CTAs x (32 + 1) complex128)
+constexpr size_t kPanelGridScratch = 176u * 1024u;
 
 template <typename C>
 int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv);
@@ -72,8 +76,10 @@ inline int gemm(const LaContext& ctx, int m, int n, int k, C alpha, const C* A, 
 
 // P A = L U in place (storage rows stay put).  rowmap: n int32 (output),
 // ipiv: n int32 (output, LAPACK swap sequence, 0-based).  scratch: 2 n ints
-// (row-map snapshots) selects the look-ahead schedule; NULL selects the
-// single-stream recursive one.  Both give the same pivots.
+// (row-map snapshots) followed by kPanelGridScratch bytes, 256-aligned,
+// selects the look-ahead schedule; NULL selects the single-stream recursive
+// one.  Both give the same pivots.  Panels of more rows than one 16-CTA
+// cluster holds (6144) need the scratch (grid-wide panel).
 template <typename C>
 int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv, int32_t* scratch);
 

@@ -172,3 +172,17 @@ def test_getrf_lookahead_c64_tensor_cores(cuda):
         getrs(At, rowmap, Bt)
         errs.append(np.max(np.abs(Bt.cpu().numpy() - X)) / np.max(np.abs(X)))
     assert errs[0] < 2e-4 and errs[0] < 3 * errs[1] + 1e-6, errs
+
+
+def test_getrf_lookahead_tall_panel_c128(cuda):
+    """n = 6500 > 6144 rows: the first panels are factored by the grid-wide
+    (cooperative) panel kernel; pivots and factors still match LAPACK."""
+    n = 6500
+    A = _rand(n, n, 2024)
+    At = _t(A)
+    rowmap, ipiv, info = _getrf_ws(At, 0)
+    lu, piv = sla.lu_factor(A)
+    assert int(info.item()) == 0
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv)
+    got = At.cpu().numpy()[rowmap.cpu().numpy()]
+    assert np.max(np.abs(got - lu)) / np.max(np.abs(lu)) < 1e-10
