@@ -226,7 +226,8 @@ class BEMRetIter:
             if self._hmat is None:
                 self._hmat = BEMHMatrices(self.p, self.g, htol=self.htol, kmax=self.kmax, cleaf=self.cleaf,
                                           eta=self.eta)
-            self._hmat.build(enei)
+            shared = bem._G128 if (self.precond is not None and bem._prec == 1) else None
+            self._hmat.build(enei, mats=shared)
         else:
             if bem._prec == 1 and self.precond is not None:
                 self._G = bem._G128  # assembled by the mixed init

@@ -292,14 +292,18 @@ class BEMHMatrices:
         self.H = None
         self.enei = None
 
-    def build(self, enei):
+    def build(self, enei, mats=None):
+        """Compress G1, G2, H1, H2 at ``enei``; ``mats`` may hand in the four
+        dense complex128 matrices already assembled at this wavelength."""
         torch = _torch()
         n = self.n
         fad = make_kaware_fadmiss(2.0 * np.pi / enei, eta0=self.eta)
         dense, low = block_partition(self.tree, fad)
         dev = self.g.device
-        mats = [torch.empty((n, n), dtype=torch.complex128, device=dev) for _ in range(4)]
-        self.g.bem_matrices(enei, dtype="c128", out=mats)
+        if mats is None:
+            mats = [torch.empty((n, n), dtype=torch.complex128, device=dev) for _ in range(4)]
+            self.g.bem_matrices(enei, dtype="c128", out=mats)
+        self.H = None
         scratch = torch.empty((n, n), dtype=torch.complex128, device=dev)
         self.H = [HMatrixGPU(self.tree, dense, low, htol=self.htol, kmax=self.kmax).compress(M, scratch) for M in mats]
         del mats, scratch

@@ -6,6 +6,7 @@
     python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1]
     python -m mnpbem_b200.microbench hmat  [--faces 1444] [--cleaf 200] [--htol 1e-6] [--reps 3]
     python -m mnpbem_b200.microbench iter  [--faces 1444] [--hmatrix] [--noprecond] [--tol 1e-10]
+    python -m mnpbem_b200.microbench large [--side 3] [--hmatrix] [--tol 1e-8]
 
 ``step`` runs whole per-wavelength solves (assembly + init + solve) of the
 sphere dimer (two trisphere(faces) spheres, 2 nm gap, water, Drude gold,
@@ -191,9 +192,52 @@ def case_iter(a):
     return out
 
 
+def sphere_array(side=3, faces=1444, diameter=40.0, gap=2.0, eps_b=1.0):
+    """side x side gold spheres (trisphere(faces, diameter)) on a square grid in
+    the xy plane with surface gaps ``gap``: 2884 side^2 faces at faces=1444."""
+    from . import ComParticle, EpsConst, EpsDrude, trisphere
+    parts = []
+    pitch = diameter + gap
+    for i in range(side):
+        for j in range(side):
+            q = trisphere(faces, diameter)
+            q.shift([(i - (side - 1) / 2) * pitch, (j - (side - 1) / 2) * pitch, 0.0])
+            parts.append(q)
+    k = len(parts)
+    return ComParticle([EpsConst(eps_b), EpsDrude(9.84, 9.0, 0.067)], parts, [[2, 1]] * k, *range(1, k + 1),
+                       interp="curv")
+
+
+def case_large(a):
+    """One large solve (3 x 3 gold spheres, 25956 faces, vacuum, 700 nm, x-pol):
+    BEMRetIter with the complex64 tensor-core LU as preconditioner and the
+    FP64 dense (or H-matrix) operator."""
+    import torch
+    from . import PlaneWaveRet
+    from .bem_iter import BEMRetIter
+    cp = sphere_array(a.side)
+    exc = PlaneWaveRet(np.array([[1.0, 0, 0]]), np.array([[0, 0, 1.0]]))
+    e0, e1, e2 = _events() + (torch.cuda.Event(enable_timing=True),)
+    torch.cuda.synchronize()
+    e0.record()
+    bem = BEMRetIter(cp, hmatrix=a.hmatrix, cleaf=a.cleaf, htol=a.htol, tol=a.tol)
+    bem.init(700.0)
+    e1.record()
+    sig, _ = bem.solve(exc.potential(cp, 700.0))
+    e2.record()
+    torch.cuda.synchronize()
+    out = {"case": "large", "faces": cp.n, "hmatrix": a.hmatrix, "tol": a.tol, "ext": exc.extinction(sig),
+           "sca": exc.scattering(sig)[0], "iters": bem.last.iter, "relres": bem.last.relres,
+           "ms_ctor_init": e0.elapsed_time(e1), "ms_solve": e1.elapsed_time(e2),
+           "max_mem_GB": torch.cuda.max_memory_allocated() / 1e9}
+    if a.hmatrix:
+        out["compression"] = bem._hmat.compression()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter"])
+    ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter", "large"])
     ap.add_argument("--faces", type=int, default=1444)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--engine", type=int, default=1)
@@ -210,6 +254,7 @@ def main(argv=None):
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--hmatrix", action="store_true")
     ap.add_argument("--noprecond", action="store_true")
+    ap.add_argument("--side", type=int, default=3)
     a = ap.parse_args(argv)
     import torch
     if not torch.cuda.is_available():
@@ -217,7 +262,7 @@ def main(argv=None):
     if a.case == "step":
         a.engine = {0: "simt", 1: "bf16x3", 2: "tf32"}[a.engine]
     out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf, "hmat": case_hmat,
-           "iter": case_iter}[a.case](a)
+           "iter": case_iter, "large": case_large}[a.case](a)
     print(json.dumps(out), flush=True)
 
 
