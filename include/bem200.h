@@ -297,6 +297,25 @@ int bem200_gmres_combine(int64_t len, int m, const void* V, const double* y_host
                          void* stream);
 int bem200_zaxpy(int64_t len, const double* a, const void* x, void* y, void* stream);
 
+/* ------------------------------------------------------------- plane wave
+ * bem200_planewave_rhs: the right-hand side b (8 n p complex128, layout of
+ * bem200_bem_solve) of p <= 8 plane waves exp(i km dir.r) with polarisations
+ * pol (HOST arrays, p x 3), km = (re, im) the wavenumber of the embedding
+ * medium (HOST); on_side (n x 2 int8) marks the face sides that touch the
+ * medium.  Replaces PlaneWaveRet.potential
+ * (mnpbem/simulation/planewave_ret.py:257-361) followed by BEMRet._excitation
+ * (mnpbem/bem/bem_ret.py:1360-1429).
+ * bem200_farfield: e, h (ndir x 3 x p complex128) far-field amplitudes on the
+ * directions dirs (ndir x 3, device) from W1 = [sig1 | h1], W2 = [sig2 | h2]
+ * (n x 4p); p <= 4.  Replaces SpectrumRet.farfield
+ * (mnpbem/spectrum/spectrum_ret.py:231-392). */
+int bem200_planewave_rhs(int n, int npol, const double* pos, const double* nvec, const int8_t* on_side,
+                         const double* pol_host, const double* dir_host, const double* km_host, double k0,
+                         int eps_per_face, const double* eps1, const double* eps2, void* b, void* stream);
+int bem200_farfield(int n, int npol, int ndir, const double* dirs, const double* pos, const double* area,
+                    const int8_t* on_side, const double* km_host, double k0, const void* W1, const void* W2,
+                    void* e_out, void* h_out, void* stream);
+
 /* dst (complex64) = src (complex128), count elements. */
 int bem200_convert_c128_c64(int64_t count, const void* src, void* dst, void* stream);
 

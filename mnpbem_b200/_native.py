@@ -78,6 +78,10 @@ _SIGS = {
                                        ctypes.c_int, ctypes.c_int, _vp]),
     "bem200_hmat_matvec": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
                                           _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "bem200_planewave_rhs": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _dbl,
+                                            ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "bem200_farfield": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _dbl, _vp,
+                                       _vp, _vp, _vp, _vp]),
     "bem200_gmres_orth_workspace_size": (_sz, [ctypes.c_int]),
     "bem200_gmres_orth": (ctypes.c_int, [_i64, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "bem200_gmres_combine": (ctypes.c_int, [_i64, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),

@@ -243,6 +243,19 @@ class BEMRet:
         sig = CompStruct(self.p, enei, sig1=sig1, sig2=sig2, h1=h1, h2=h2)
         return sig, self
 
+    def cross_sections(self, exc, enei):
+        """Extinction and scattering of a plane wave at ``enei`` with every
+        per-wavelength step on the GPU: the right-hand side, the solve and the
+        far fields; only the cross sections come back.  Returns dict ext, sca
+        ((npol,) arrays)."""
+        self.init(enei)
+        bt, npol = exc.rhs_device(self.p, enei, self._eps_mode, self._e1p, self._e2p, device=self.dev)
+        W1, W2 = self.solve_device(bt, npol)
+        if self._prec == 0:
+            self.check_status()
+        ext, sca, _ = exc.cross_sections_device(self.p, enei, W1, W2)
+        return {"ext": ext, "sca": sca}
+
     def __truediv__(self, exc):
         """``bem / exc`` -> sig (MATLAB ``bem \\ exc``)."""
         return self.solve(exc)[0]

@@ -91,6 +91,31 @@ class SpectrumRet:
         return sca, dsca
 
 
+def _on_side(p, medium, device):
+    """(n, 2) int8 device mask: face side s faces the embedding medium."""
+    import torch
+    key = (id(p), medium, str(device))
+    cache = getattr(p, "_b200_side_cache", None)
+    if cache is not None and cache[0] == key:
+        return cache[1]
+    io = np.asarray(p.inout_faces)
+    m = torch.as_tensor(np.ascontiguousarray((io == medium).astype(np.int8)), device=device)
+    p._b200_side_cache = (key, m)
+    return m
+
+
+def _face_tensors(p, device):
+    import torch
+    cache = getattr(p, "_b200_face_cache", None)
+    if cache is not None and cache[0] == str(device):
+        return cache[1]
+    f64 = dict(dtype=torch.float64, device=device)
+    t = (torch.as_tensor(np.ascontiguousarray(p.pos), **f64), torch.as_tensor(np.ascontiguousarray(p.nvec), **f64),
+         torch.as_tensor(np.ascontiguousarray(p.area), **f64))
+    p._b200_face_cache = (str(device), t)
+    return t
+
+
 class PlaneWaveRet:
     """Plane wave exp(i k dir.r) with polarisation pol (one row per excitation)."""
 
@@ -130,6 +155,62 @@ class PlaneWaveRet:
         return exc
 
     __call__ = potential
+
+    def rhs_device(self, p, enei, eps_mode, e1p, e2p, device="cuda"):
+        """The BEM right-hand side of this plane wave directly on the device
+        (8 n npol complex128, layout of BEMRet.rhs): potential() fused with the
+        excitation of BEMRet (planewave_ret.py:257-361, bem_ret.py:1360-1429).
+        eps_mode / e1p / e2p: the eps arguments of the C ABI."""
+        import ctypes
+        import torch
+        from . import _native as nat
+        if not np.allclose(np.sum(self.pol * self.dir, axis=1), 0):
+            raise ValueError("PlaneWaveRet: polarisation and direction must be orthogonal")
+        npol = self.pol.shape[0]
+        eps_val = complex(np.asarray(p.eps[self.medium - 1](enei)[0]).ravel()[0])
+        k0 = 2 * np.pi / enei
+        km = k0 * np.sqrt(eps_val)
+        pos, nvec, _ = _face_tensors(p, device)
+        side = _on_side(p, self.medium, device)
+        b = torch.empty(8 * p.n * npol, dtype=torch.complex128, device=device)
+        pol = (ctypes.c_double * (3 * npol))(*self.pol.ravel())
+        dirs = (ctypes.c_double * (3 * npol))(*self.dir.ravel())
+        kmh = (ctypes.c_double * 2)(km.real, km.imag)
+        nat.call("bem200_planewave_rhs", p.n, npol, nat.ptr(pos), nat.ptr(nvec), nat.ptr(side), pol, dirs, kmh, k0,
+                 eps_mode, e1p, e2p, nat.ptr(b), nat.stream_ptr())
+        return b, npol
+
+    def cross_sections_device(self, p, enei, W1, W2):
+        """Extinction and scattering from device solutions W1 = [sig1 | h1],
+        W2 = [sig2 | h2] (n x 4 npol): far fields on the GPU, the O(ndir)
+        sums on the host.  Returns (ext (npol,), sca (npol,), dsca (ndir, npol))."""
+        import ctypes
+        import torch
+        from . import _native as nat
+        npol = self.pol.shape[0]
+        dev = W1.device
+        km = complex(np.asarray(p.eps[self.medium - 1](enei)[1]).ravel()[0])
+        k0 = 2 * np.pi / enei
+        pos, _, area = _face_tensors(p, dev)
+        side = _on_side(p, self.medium, dev)
+        spec = self.spec
+        if getattr(spec, "_dev_dirs", None) is None or spec._dev_dirs.device != dev:
+            spec._dev_dirs = torch.as_tensor(np.ascontiguousarray(np.vstack([spec.nvec, self.dir])), device=dev)
+        nd = spec._dev_dirs.shape[0]
+        e = torch.empty((nd, 3, npol), dtype=torch.complex128, device=dev)
+        h = torch.empty_like(e)
+        kmh = (ctypes.c_double * 2)(km.real, km.imag)
+        nat.call("bem200_farfield", p.n, npol, nd, nat.ptr(spec._dev_dirs), nat.ptr(pos), nat.ptr(area), nat.ptr(side),
+                 kmh, k0, nat.ptr(W1), nat.ptr(W2), nat.ptr(e), nat.ptr(h), nat.stream_ptr())
+        e, h = e.cpu().numpy(), h.cpu().numpy()
+        ns = spec.ndir
+        dsca = 0.5 * np.real(np.einsum("dc,dcp->dp", spec.nvec, np.cross(e[:ns], np.conj(h[:ns]), axis=1)))
+        nb = np.real(np.sqrt(complex(np.asarray(p.eps[self.medium - 1](enei)[0]).ravel()[0])))
+        sca = (spec.area @ dsca) / (0.5 * nb)
+        einc = e[ns:]
+        pe = np.array([np.sum(np.conj(self.pol[i]) * einc[i, :, i]) for i in range(npol)])
+        ext = np.real(4 * np.pi / km * np.imag(pe))
+        return ext, sca, dsca / (0.5 * nb)
 
     def extinction(self, sig):
         """Optical theorem (planewave_ret.py:437-504)."""
