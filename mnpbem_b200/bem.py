@@ -105,7 +105,9 @@ class BEMRet:
         slots = [ctypes.c_void_p() for _ in range(4)]
         nat.call("bem200_bem_slots", prec, n, nat.ptr(self._ws), *[ctypes.byref(s) for s in slots])
         self._slots = [s.value for s in slots]
-        gbytes = int(L.bem200_gemm_workspace_size(_ENGINES[self.engine], n, n, n))
+        # operand space of the largest GEMM plus headroom for the concurrent
+        # halves of the factor chains (each needs about a quarter of it)
+        gbytes = int(L.bem200_gemm_workspace_size(_ENGINES[self.engine], n, n, n) * 5 // 4)
         self._gws = torch.empty(max(gbytes, 1), dtype=torch.uint8, device=self.dev)
         self._gws_bytes = gbytes
         self._nvec = torch.as_tensor(np.ascontiguousarray(p.nvec), dtype=torch.float64, device=self.dev)

@@ -1564,8 +1564,33 @@ int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld,
 }
 
 template <typename C>
+static int solve_right_rows(const LaContext& ctx, int n, int m, const C* LU, long long ld, const int32_t* rowmap,
+                            C* X, long long ldx, C* tmp);
+
+// rows of X are independent: with enough workspace, the second half of the
+// rows runs on a forked stream (the narrow deep-recursion GEMMs of the two
+// halves then share the GPU)
+template <typename C>
 int solve_right(const LaContext& ctx, int n, int m, const C* LU, long long ld, const int32_t* rowmap, C* X,
                 long long ldx, C* tmp) {
+  const int h = m / 2;
+  const bool split = m >= 1024 && (ctx.engine == GemmEngine::kSimt ||
+                                   gemm_tc_workspace(m - h, n / 2 + 64, n / 2 + 64, ctx.engine) <= ctx.ws_bytes / 2);
+  if (!split) return solve_right_rows<C>(ctx, n, m, LU, ld, rowmap, X, ldx, tmp);
+  LaContext c1 = ctx, c2;
+  SideStream ss;
+  BEM_REQUIRE(ss.fork(c1, c2), BEM200_ERR_CUDA, "solve_right: could not fork a stream");
+  int st = solve_right_rows<C>(c1, n, h, LU, ld, rowmap, X, ldx, tmp);
+  if (st) return st;
+  st = solve_right_rows<C>(c2, n, m - h, LU, ld, rowmap, X + (long long)h * ldx, ldx, tmp + (long long)h * n);
+  if (st) return st;
+  BEM_CUDA_CHECK(ss.join(ctx.stream));
+  return BEM200_OK;
+}
+
+template <typename C>
+static int solve_right_rows(const LaContext& ctx, int n, int m, const C* LU, long long ld, const int32_t* rowmap,
+                            C* X, long long ldx, C* tmp) {
   // X A = Y with P A = L U  =>  X = Y U^-1 L^-1 P
   if (m <= 0) return BEM200_OK;
   RowView<C> T{const_cast<C*>(LU), ld, rowmap, 0};
@@ -1595,9 +1620,26 @@ int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_
   perm_matrix_kernel<C><<<ceil_div((long long)n * n, 256), 256, 0, ctx.stream>>>(n, rowmap, Inv, ldi);
   BEM_LAUNCH_CHECK();
   RowView<C> T{const_cast<C*>(LU), ld, rowmap, 0};
-  int st = trsm_llu<C>(ctx, n, n, T, plain(Inv, ldi));
-  if (st) return st;
-  return trsm_lun<C>(ctx, n, n, T, plain(Inv, ldi));
+  // the columns of the inverse are independent: with enough workspace the
+  // second half of them is solved on a forked stream
+  const int h = n / 2;
+  const bool split = n >= 1024 && (ctx.engine == GemmEngine::kSimt ||
+                                   gemm_tc_workspace(n, n - h + 64, n, ctx.engine) <= ctx.ws_bytes / 2);
+  if (!split) {
+    int st = trsm_llu<C>(ctx, n, n, T, plain(Inv, ldi));
+    if (st) return st;
+    return trsm_lun<C>(ctx, n, n, T, plain(Inv, ldi));
+  }
+  LaContext c1 = ctx, c2;
+  SideStream ss;
+  BEM_REQUIRE(ss.fork(c1, c2), BEM200_ERR_CUDA, "inverse: could not fork a stream");
+  int st;
+  if ((st = trsm_llu<C>(c1, n, h, T, plain(Inv, ldi)))) return st;
+  if ((st = trsm_llu<C>(c2, n, n - h, T, plain(Inv + h, ldi)))) return st;
+  if ((st = trsm_lun<C>(c1, n, h, T, plain(Inv, ldi)))) return st;
+  if ((st = trsm_lun<C>(c2, n, n - h, T, plain(Inv + h, ldi)))) return st;
+  BEM_CUDA_CHECK(ss.join(ctx.stream));
+  return BEM200_OK;
 }
 
 // explicit instantiations

@@ -64,6 +64,42 @@ struct LaContext {
 // bytes of the grid-wide panel's candidate slots (2 x up to 160 CTAs x (32 + 1) complex128)
 constexpr size_t kPanelGridScratch = 176u * 1024u;
 
+// A non-blocking side stream forked from ctx.stream (fork()) and joined back
+// into it (join()); the destructor releases the stream and events once their
+// queued work has finished.  The side context gets the upper half of the
+// tensor-core operand workspace, the main one keeps the lower half.
+struct SideStream {
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  ~SideStream() {
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
+  }
+  // splits the workspace of `main`; returns false (nothing forked) on failure
+  bool fork(LaContext& main, LaContext& aux) {
+    if (cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess) return false;
+    if (cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess) return false;
+    if (cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess) return false;
+    if (cudaEventRecord(ev_fork, main.stream) != cudaSuccess) return false;
+    if (cudaStreamWaitEvent(side, ev_fork, 0) != cudaSuccess) return false;
+    aux = main;
+    aux.stream = side;
+    if (main.engine != GemmEngine::kSimt) {
+      const size_t h = (main.ws_bytes / 2) & ~size_t(255);
+      main.ws_bytes = h;
+      aux.ws = reinterpret_cast<char*>(main.ws) + h;
+      aux.ws_bytes = h;
+    }
+    return true;
+  }
+  cudaError_t join(cudaStream_t main_stream) {
+    cudaError_t e = cudaEventRecord(ev_join, side);
+    if (e != cudaSuccess) return e;
+    return cudaStreamWaitEvent(main_stream, ev_join, 0);
+  }
+};
+
 template <typename C>
 int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv);
 

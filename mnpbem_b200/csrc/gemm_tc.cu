@@ -208,28 +208,51 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_bf16x3_kernel(const __grid_co
     umma_commit(&acc_bar);  // accumulator complete (or abandoned)
   } else if (warp >= 4) {
     // ---------------- epilogue: TMEM -> alpha/beta -> complex64 stores
+    // Each thread of an epilogue warp owns one TMEM lane (one output row).  A
+    // 16-column chunk is staged through shared memory (the pipeline stages are
+    // idle once the accumulator is complete) and written back transposed, so
+    // that 16 lanes store 128 contiguous bytes of one row.
     const int ew = warp - 4;  // TMEM lanes 32 ew .. 32 ew + 31
     bool ok = mbar_wait(&acc_bar, 0, args.status);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int row = tile_m * BM + ew * 32 + lane;
-    const bool row_ok = ok && !abort_sh && row < args.m;
-    float2* crow = row_ok ? args.C.base + args.C.off(row, 0) : nullptr;
+    const bool tile_ok = ok && !abort_sh;
+    float2(*stage)[17] = reinterpret_cast<float2(*)[17]>(base + ew * 32 * 17 * sizeof(float2));
     const bool use_beta = (args.beta.x != 0.f || args.beta.y != 0.f);
     const int q0 = tile_n * (BN / 2);
+    const int row_base = tile_m * BM + ew * 32;
+    const int half = lane >> 4, j = lane & 15;
+    // element offset of this lane's row (row maps are read once per row)
+    const long long my_off = (row_base + lane < args.m) ? args.C.off(row_base + lane, 0) : 0;
+    const int nrows = min(32, args.m - row_base);
 #pragma unroll 1
     for (int cb = 0; cb < BN / 32; ++cb) {
       uint32_t r[32];
       tmem_ld32(tmem + ((uint32_t)(ew * 32) << 16) + cb * 32, r);  // all lanes take part
-      if (!row_ok) continue;
+      if (!tile_ok || nrows <= 0) continue;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int q = q0 + cb * 16 + j;
-        if (q >= args.n) break;
-        float2 acc = make_float2(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
-        float2 v = cmul(args.alpha, acc);
-        if (use_beta) v = cadd(v, cmul(args.beta, crow[q]));
-        crow[q] = v;
+      for (int jj = 0; jj < 16; ++jj) stage[lane][jj] = make_float2(__uint_as_float(r[2 * jj]), __uint_as_float(r[2 * jj + 1]));
+      __syncwarp();
+      const int q = q0 + cb * 16 + j;
+      const bool qok = q < args.n;
+      long long ro[16];
+      float2 cv[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) ro[i] = __shfl_sync(0xffffffffu, my_off, 2 * i + half);
+      if (use_beta) {  // all 16 loads of C in flight before the first store
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          cv[i] = (qok && 2 * i + half < nrows) ? args.C.base[ro[i] + q] : make_float2(0.f, 0.f);
       }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int rr = 2 * i + half;
+        if (qok && rr < nrows) {
+          float2 v = cmul(args.alpha, stage[rr][j]);
+          if (use_beta) v = cadd(v, cmul(args.beta, cv[i]));
+          args.C.base[ro[i] + q] = v;
+        }
+      }
+      __syncwarp();
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
