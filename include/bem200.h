@@ -126,6 +126,18 @@ int bem200_green_assemble(int n, int npart, const int32_t* pid, const int32_t* b
                           const double* g, const double* fn, int out_dtype, void* G1, void* G2,
                           void* H1, void* H2, int64_t ld, void* stream);
 
+/* d/dk of G1, G2, H1, H2 (complex128) for the wavenumber of material dmat
+ * (1-based, <= nmat): the region terms filled with that material, far
+ * entries dG/dk = i d G, dF/dk = -k d (n.r) area / d^2 e^{ikd}, refined
+ * entries i sum_m c_m (m (ik)^(m-1) + d (ik)^m) e^{ikd}.  The tangent of the
+ * BEM operator for derivatives with respect to a material's permittivity
+ * (no counterpart call in the reference, which has no gradients). */
+int bem200_green_assemble_dk(int n, int npart, const int32_t* pid, const int32_t* blk_mat, int nmat,
+                             const double* kmat_host, int dmat, const double* pos, const double* nvec,
+                             const double* area, int64_t nref, const int32_t* ref_row, const int32_t* ref_col,
+                             int order, const double* g, const double* fn, void* G1, void* G2, void* H1, void* H2,
+                             int64_t ld, void* stream);
+
 /* ------------------------------------------------------------- dense LA
  * Building blocks of the dense BEM (reference: the LU / lu_solve / matmul
  * calls of mnpbem/bem/bem_ret.py:437-523, dispatched through

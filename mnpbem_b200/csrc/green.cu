@@ -647,6 +647,122 @@ __global__ void green_refined_kernel(long long nref, const int32_t* __restrict__
   if (H2) store_c<C>(H2, idx, out[6], out[7]);
 }
 
+// ----------------------------------------------------------- d/dk of (a6)
+// Derivatives of the four BEM matrices with respect to the wavenumber of one
+// material `dmat` (1-based): only region terms filled with that material
+// contribute (the 2 pi diagonal terms are constant).
+//   far:      dG/dk = i d G,   dF/dk = -k d F_pre e^{ikd}  (F_pre = (n.r) area / d^2)
+//   refined:  d/dk [sum_m c_m (ik)^m e^{ikd}] = sum_m c_m [i m (ik)^(m-1) + i d (ik)^m] e^{ikd}
+template <typename C>
+__global__ void __launch_bounds__(kAsmThreads) green_far_dk_kernel(
+    int n, int npart, int dmat, const int32_t* __restrict__ pid, const int32_t* __restrict__ blk_mat, KTable kt,
+    const double* __restrict__ pos, const double* __restrict__ nvec, const double* __restrict__ area, void* G1,
+    void* G2, void* H1, void* H2, long long ld) {
+  const int j = blockIdx.x * kAsmThreads + threadIdx.x;
+  const int i0 = blockIdx.y * kRowsPerBlock;
+  if (j >= n) return;
+  const double3 pj = ld3(pos, j);
+  const double aj = area[j];
+  const int bj = pid[j];
+  const int rows = min(kRowsPerBlock, n - i0);
+  for (int r = 0; r < rows; ++r) {
+    const int i = i0 + r;
+    const int bi = pid[i];
+    const double3 rv = sub3(ld3(pos, i), pj);
+    const bool diag = (bi == bj) && (i == j);
+    const double d = diag ? kEps : fmax(norm3(rv), kEps);
+    const double ndr = dot3(ld3(nvec, i), rv);
+    const int* bm = blk_mat + (bi * npart + bj) * 4;
+    const double gpre = aj / d, fpre = ndr / (d * d) * aj;
+    double out[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) out[q] = 0.0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      if (bm[t] != dmat) continue;
+      const double kr = kt.re[dmat - 1], ki = kt.im[dmat - 1];
+      double pr, pim;
+      phase(kr, ki, d, pr, pim);
+      // dG/dk = i d gpre e^{ikd};  dF/dk = -k d fpre e^{ikd}
+      const double gr = -d * gpre * pim, gi = d * gpre * pr;
+      const double kdr = kr * d * fpre, kdi = ki * d * fpre;  // k d fpre
+      const double fr = -(kdr * pr - kdi * pim), fi = -(kdr * pim + kdi * pr);
+      const double sgn = (t == 0 || t == 2) ? 1.0 : -1.0;
+      const int oG = (t < 2) ? 0 : 2, oH = (t < 2) ? 4 : 6;
+      out[oG] += sgn * gr;
+      out[oG + 1] += sgn * gi;
+      out[oH] += sgn * fr;
+      out[oH + 1] += sgn * fi;
+    }
+    const long long idx = (long long)i * ld + j;
+    if (G1) store_c<C>(G1, idx, out[0], out[1]);
+    if (G2) store_c<C>(G2, idx, out[2], out[3]);
+    if (H1) store_c<C>(H1, idx, out[4], out[5]);
+    if (H2) store_c<C>(H2, idx, out[6], out[7]);
+  }
+}
+
+template <typename C>
+__global__ void green_refined_dk_kernel(long long nref, int dmat, const int32_t* __restrict__ ref_row,
+                                        const int32_t* __restrict__ ref_col, int order, const double* __restrict__ g,
+                                        const double* __restrict__ fn, int npart, const int32_t* __restrict__ pid,
+                                        const int32_t* __restrict__ blk_mat, KTable kt, const double* __restrict__ pos,
+                                        void* G1, void* G2, void* H1, void* H2, long long ld) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nref) return;
+  const int i = ref_row[e], j = ref_col[e];
+  const int bi = pid[i], bj = pid[j];
+  const bool diag = (bi == bj) && (i == j);
+  const double d = diag ? kEps : fmax(norm3(sub3(ld3(pos, i), ld3(pos, j))), kEps);
+  const int no = order + 1;
+  const int* bm = blk_mat + (bi * npart + bj) * 4;
+  double out[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) out[q] = 0.0;
+  for (int t = 0; t < 4; ++t) {
+    if (bm[t] != dmat) continue;
+    const double kr = kt.re[dmat - 1], ki = kt.im[dmat - 1];
+    // S = sum c_m (ik)^m,  S' = sum c_m m (ik)^(m-1)   (ik = -ki + i kr)
+    double pr_ = 1.0, pi_ = 0.0, qr = 0.0, qi = 0.0;  // (ik)^m and (ik)^(m-1)
+    double Gr = 0, Gi = 0, Fr = 0, Fi = 0, dGr = 0, dGi = 0, dFr = 0, dFi = 0;
+    for (int q = 0; q < no; ++q) {
+      const double gq = g[e * no + q], fq = fn[e * no + q];
+      Gr += gq * pr_;
+      Gi += gq * pi_;
+      Fr += fq * pr_;
+      Fi += fq * pi_;
+      dGr += gq * q * qr;
+      dGi += gq * q * qi;
+      dFr += fq * q * qr;
+      dFi += fq * q * qi;
+      qr = pr_;
+      qi = pi_;
+      const double nr = pr_ * (-ki) - pi_ * kr, ni = pr_ * kr + pi_ * (-ki);
+      pr_ = nr;
+      pi_ = ni;
+    }
+    // d/dk = i [S' + d S] e^{ikd}
+    double ph_r, ph_i;
+    phase(kr, ki, d, ph_r, ph_i);
+    const double sgr = dGr + d * Gr, sgi = dGi + d * Gi;
+    const double sfr = dFr + d * Fr, sfi = dFi + d * Fi;
+    const double igr = -sgi, igi = sgr, ifr = -sfi, ifi = sfr;  // multiply by i
+    const double gr = igr * ph_r - igi * ph_i, gi = igr * ph_i + igi * ph_r;
+    const double fr = ifr * ph_r - ifi * ph_i, fi = ifr * ph_i + ifi * ph_r;
+    const double sgn = (t == 0 || t == 2) ? 1.0 : -1.0;
+    const int oG = (t < 2) ? 0 : 2, oH = (t < 2) ? 4 : 6;
+    out[oG] += sgn * gr;
+    out[oG + 1] += sgn * gi;
+    out[oH] += sgn * fr;
+    out[oH + 1] += sgn * fi;
+  }
+  const long long idx = (long long)i * ld + j;
+  if (G1) store_c<C>(G1, idx, out[0], out[1]);
+  if (G2) store_c<C>(G2, idx, out[2], out[3]);
+  if (H1) store_c<C>(H1, idx, out[4], out[5]);
+  if (H2) store_c<C>(H2, idx, out[6], out[7]);
+}
+
 }  // namespace bem200
 
 using namespace bem200;
@@ -783,6 +899,35 @@ int bem200_green_assemble(int n, int npart, const int32_t* pid, const int32_t* b
     else
       green_refined_kernel<float2><<<ceil_div(nref, 256), 256, 0, s>>>(nref, ref_row, ref_col, order, g, fn, npart,
                                                                         pid, blk_mat, kt, pos, G1, G2, H1, H2, ld);
+    BEM_LAUNCH_CHECK();
+  }
+  return BEM200_OK;
+}
+
+int bem200_green_assemble_dk(int n, int npart, const int32_t* pid, const int32_t* blk_mat, int nmat,
+                             const double* kmat_host, int dmat, const double* pos, const double* nvec,
+                             const double* area, int64_t nref, const int32_t* ref_row, const int32_t* ref_col,
+                             int order, const double* g, const double* fn, void* G1, void* G2, void* H1, void* H2,
+                             int64_t ld, void* stream) {
+  BEM_REQUIRE(n > 0 && npart > 0 && ld >= n && nmat > 0 && nmat <= kMaxMat && kmat_host && dmat >= 1 &&
+                  dmat <= nmat && pid && blk_mat && pos && nvec && area && order >= 0 && order <= kMaxOrder,
+              BEM200_ERR_ARG, "green_assemble_dk: bad arguments");
+  KTable kt;
+  for (int m = 0; m < kMaxMat; ++m) {
+    kt.re[m] = m < nmat ? kmat_host[2 * m] : 0.0;
+    kt.im[m] = m < nmat ? kmat_host[2 * m + 1] : 0.0;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  dim3 grid(ceil_div(n, kAsmThreads), ceil_div(n, kRowsPerBlock));
+  BEM_REQUIRE(grid.y <= 65535, BEM200_ERR_ARG, "green_assemble_dk: n too large");
+  green_far_dk_kernel<double2><<<grid, kAsmThreads, 0, s>>>(n, npart, dmat, pid, blk_mat, kt, pos, nvec, area, G1, G2,
+                                                             H1, H2, ld);
+  BEM_LAUNCH_CHECK();
+  if (nref > 0) {
+    BEM_REQUIRE(ref_row && ref_col && g && fn, BEM200_ERR_ARG, "green_assemble_dk: null refinement arrays");
+    green_refined_dk_kernel<double2><<<ceil_div(nref, 256), 256, 0, s>>>(nref, dmat, ref_row, ref_col, order, g, fn,
+                                                                          npart, pid, blk_mat, kt, pos, G1, G2, H1,
+                                                                          H2, ld);
     BEM_LAUNCH_CHECK();
   }
   return BEM200_OK;
