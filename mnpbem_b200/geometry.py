@@ -119,7 +119,7 @@ class Particle:
         self.quad = QuadFace(rule=kwargs.get("rule", 18), npol=kwargs.get("npol", (7, 5)),
                              refine=kwargs.get("refine", None))
         self.interp = interp
-        if norm and len(self.faces) > 0:
+        if norm not in (False, "off") and len(self.faces) > 0:
             self._norm()
         else:
             self.pos = np.zeros((0, 3))
@@ -426,6 +426,78 @@ class Particle:
         new._norm()
         return new
 
+    def flip(self, dir=0):
+        """Mirror copy along the axes ``dir`` (0, 1, 2 or a list), faces
+        reoriented so the normals stay outward (reference particle.py:843-866)."""
+        new = copy.deepcopy(self)
+        for d in ([dir] if np.isscalar(dir) else list(dir)):
+            new.verts[:, d] = -new.verts[:, d]
+            if new.verts2 is not None:
+                new.verts2[:, d] = -new.verts2[:, d]
+        return new.flipfaces()
+
+    def clean(self, cutoff=1e-10):
+        """Merge vertices equal to 8 decimals, turn quads with a repeated corner
+        into triangles and drop faces of area <= cutoff * mean area
+        (reference particle.py:2331-2395).
+
+        As in the reference, the merged corner vertices take their rounded
+        coordinates and the curved-node table (verts2, faces2) is left as it
+        is; only the face selection touches it."""
+        vr = mround(self.verts, 8)
+        uniq, inv = np.unique(vr, axis=0, return_inverse=True)
+        inv = inv.ravel()
+        if len(uniq) != len(self.verts):
+            f = self.faces.copy()
+            ok = ~np.isnan(f)
+            f[ok] = inv[f[ok].astype(int)]
+            self.verts, self.faces = uniq, f
+        for i in np.flatnonzero(~np.isnan(self.faces[:, 3])):
+            v = self.faces[i, :4].astype(int)
+            _, first = np.unique(v, return_index=True)
+            if len(first) == 3:
+                self.faces[i] = np.append(v[np.sort(first)], np.nan)
+        self._norm()
+        keep = np.flatnonzero(self.area > cutoff * np.mean(self.area))
+        if len(keep) < self.nfaces:
+            sel = self._compress(keep)
+            self.verts, self.faces, self.verts2, self.faces2 = sel.verts, sel.faces, sel.verts2, sel.faces2
+            self._norm()
+        return self
+
+    def select(self, index=None, carfun=None):
+        """(selected, complement) particles by face index or by a predicate on
+        the centroids (reference particle.py:910-962, index / carfun forms)."""
+        if index is not None:
+            idx = np.asarray(index, dtype=int)
+        elif carfun is not None:
+            idx = np.flatnonzero(carfun(self.pos[:, 0], self.pos[:, 1], self.pos[:, 2]))
+        else:
+            raise ValueError("select: give 'index' or 'carfun'")
+        return self._compress(idx), self._compress(np.setdiff1d(np.arange(self.nfaces), idx))
+
+    def _compress(self, idx):
+        """Faces ``idx`` with unused vertices removed (reference particle.py:964-999)."""
+        if len(idx) == 0:
+            return Particle(np.zeros((0, 3)), np.zeros((0, 4)))
+
+        def renumber(faces, verts):
+            ok = ~np.isnan(faces)
+            used = np.unique(faces[ok].astype(int))
+            table = np.zeros(len(verts), dtype=int)
+            table[used] = np.arange(len(used))
+            faces = faces.copy()
+            faces[ok] = table[faces[ok].astype(int)]
+            return faces, verts[used]
+
+        f, v = renumber(self.faces[idx], self.verts)
+        new = Particle(v, f, interp=self.interp, norm=False)
+        if self.verts2 is not None and self.faces2 is not None:
+            new.faces2, new.verts2 = renumber(self.faces2[idx], self.verts2)
+        new.quad = self.quad
+        new._norm()
+        return new
+
     def curved(self, key="flat"):
         if self.verts2 is None:
             self.midpoints()
@@ -569,6 +641,161 @@ def trisphere(n, diameter=1.0, **kwargs):
     kw = dict(kwargs)
     kw.setdefault("interp", "curv")
     return Particle(v2, p.faces2, **kw)
+
+
+def mlinspace(a, b, n):
+    """a + i (b - a) / (n - 1) with the last point exactly b: MATLAB's
+    linspace, which differs from numpy's in the last bits
+    (reference mnpbem/utils/matlab_compat.py:178-194)."""
+    a, b, n = float(a), float(b), int(n)
+    if n <= 0:
+        return np.zeros(0)
+    if n == 1:
+        return np.array([b])
+    y = a + np.arange(n, dtype=float) * (b - a) / (n - 1)
+    y[-1] = b
+    return y
+
+
+def mround(x, digits=0):
+    """Round half away from zero to ``digits`` decimals (MATLAB round;
+    reference mnpbem/utils/matlab_compat.py:303-321)."""
+    x = np.asarray(x, dtype=float)
+    if digits == 0:
+        return np.trunc(x + np.copysign(0.5, x))
+    s = 10.0 ** digits
+    return mround(x * s, 0) / s
+
+
+def _fibonacci_sphere(n):
+    """n points on the unit sphere along the golden-angle spiral
+    (reference mesh_generators.py:341-370)."""
+    t = np.arange(n, dtype=float) + 0.5
+    lat = np.arccos(1 - 2 * t / n)
+    lon = np.pi * (1 + 5 ** 0.5) * t
+    p = np.column_stack([np.sin(lat) * np.cos(lon), np.sin(lat) * np.sin(lon), np.cos(lat)])
+    return p / np.linalg.norm(p, axis=1, keepdims=True)
+
+
+def _sphere_triangulate(verts):
+    """Triangulate points on the unit sphere: rotate point 0 to the south pole,
+    project the others stereographically onto z = 0, Delaunay-triangulate the
+    plane (outward winding), and close the hole with a fan from point 0 over
+    the convex hull (reference mesh_generators.py:373-443, MATLAB
+    sphtriangulate)."""
+    from scipy.spatial import ConvexHull, Delaunay
+    c = verts[0]
+    r3 = -c
+    r2 = np.array([0.0, -r3[2], r3[1]]) if c[2] != 0 else np.array([-r3[1], r3[0], 0.0])
+    r2 = r2 / np.linalg.norm(r2)
+    rot = np.array([np.cross(r3, r2), r2, r3])
+    vr = verts[1:] @ rot.T
+    s = -1.0 / (vr[:, 2] + 1)
+    plane = np.column_stack([vr[:, 0] * s, vr[:, 1] * s])
+    tri = Delaunay(plane).simplices.copy()
+    p3 = np.column_stack([plane, np.zeros(len(plane))])
+    w = np.cross(p3[tri[:, 0]] - p3[tri[:, 1]], p3[tri[:, 2]] - p3[tri[:, 1]])
+    up = w[:, 2] > 0
+    tri[up] = tri[up][:, [0, 2, 1]]
+    hull = ConvexHull(plane).vertices
+    fan = np.column_stack([np.roll(hull, -1) + 1, hull + 1, np.zeros(len(hull), dtype=hull.dtype)])
+    return np.vstack([tri + 1, fan])
+
+
+def triellipsoid(n, axes):
+    """Flat triangulated ellipsoid with about n vertices on a Fibonacci
+    spiral, semi-axes ``axes`` (reference mesh_generators.py:446-473)."""
+    v = _fibonacci_sphere(int(n))
+    f = _sphere_triangulate(v)
+    return Particle(v * np.asarray(axes, dtype=float), f)
+
+
+def _surf2patch(x, y, z, triangles=False):
+    """Faces and vertices of an (m, n) parametric grid, vertices in column-major
+    order; quads [v00 v01 v11 v10] per cell, or all first triangles
+    [v00 v01 v11] then all second ones [v00 v11 v10] (MATLAB surf2patch;
+    reference mesh_generators.py:476-511)."""
+    m, n = x.shape
+    verts = np.column_stack([x.ravel(order="F"), y.ravel(order="F"), z.ravel(order="F")])
+    i, j = np.meshgrid(np.arange(m - 1), np.arange(n - 1))
+    i, j = i.ravel(), j.ravel()          # j outer, i inner
+    v00, v10, v01, v11 = j * m + i, j * m + i + 1, (j + 1) * m + i, (j + 1) * m + i + 1
+    if triangles:
+        faces = np.vstack([np.column_stack([v00, v01, v11]), np.column_stack([v00, v11, v10])])
+    else:
+        faces = np.column_stack([v00, v01, v11, v10])
+    return faces, verts
+
+
+def fvgrid(x, y, triangles=False):
+    """Curved-node table (verts2, faces2) of the flat grid x by y in the z = 0
+    plane, faces in reversed surf2patch order (MATLAB fvgrid; reference
+    mesh_generators.py:515-544)."""
+    x, y = np.asarray(x, dtype=float), np.asarray(y, dtype=float)
+    if x.ndim == 1 and y.ndim == 1:
+        x, y = np.meshgrid(x, y)
+    faces, verts = _surf2patch(x, y, np.zeros_like(x), triangles)
+    p = Particle(verts, faces[:, ::-1], norm=False)
+    p.midpoints()
+    return p.verts2, p.faces2
+
+
+def trispheresegment(phi, theta, diameter=1.0, triangles=False, **kwargs):
+    """Sphere segment over the (phi, theta) grid with curved nodes on the
+    sphere (reference mesh_generators.py:549-585)."""
+    ph, th = np.meshgrid(np.asarray(phi, dtype=float), np.asarray(theta, dtype=float))
+    r = 0.5 * diameter
+    faces, verts = _surf2patch(r * np.sin(th) * np.cos(ph), r * np.sin(th) * np.sin(ph), r * np.cos(th), triangles)
+    p = Particle(verts, faces).clean()
+    p.midpoints()
+    nrm = np.maximum(np.sqrt(np.sum(p.verts2 ** 2, axis=1, keepdims=True)), 1e-30)
+    return Particle(r * (p.verts2 / nrm), p.faces2, **kwargs)
+
+
+def trirod(diameter, height, n=None, triangles=False, **kwargs):
+    """Rod (cylinder with hemispherical caps) along z: n = [nphi, ntheta, nz]
+    grid points around, over each cap and along the cylinder
+    (reference mesh_generators.py:592-640)."""
+    nphi, ntheta, nz = [15, 20, 20] if n is None else list(n)
+    phi = mlinspace(0, 2 * np.pi, nphi)
+    theta = mlinspace(0, 0.5 * np.pi, ntheta)
+    cap1 = trispheresegment(phi, theta, diameter, triangles=triangles, **kwargs)
+    cap1.shift([0, 0, 0.5 * (height - diameter)])
+    cap2 = cap1.flip(2)
+    v2, f2 = fvgrid(phi, 0.5 * mlinspace(-1, 1, nz) * (height - diameter), triangles=triangles)
+    r = 0.5 * diameter
+    cyl = Particle(np.column_stack([r * np.cos(v2[:, 0]), r * np.sin(v2[:, 0]), v2[:, 1]]), f2, **kwargs)
+    return (cap1 + cap2 + cyl).clean()
+
+
+def tricube(n, length=1.0, e=0.25, **kwargs):
+    """Cube with rounded edges: six n x n quad grids on the faces of the unit
+    cube, graded with the exponent e, mapped onto the super-sphere
+    |x|^(2/e) + ... and scaled to ``length`` (reference
+    mesh_generators.py:643-702). It has 6 (n - 1)^2 quadrilateral faces."""
+    length = np.asarray(length, dtype=float).ravel()
+    length = np.full(3, length[0]) if length.size != 3 else length
+    u = mlinspace(-0.5 ** e, 0.5 ** e, n)
+    v2, faces = fvgrid(u, u)
+    x = np.sign(v2[:, 0]) * np.abs(v2[:, 0]) ** (1.0 / e)
+    y = np.sign(v2[:, 1]) * np.abs(v2[:, 1]) ** (1.0 / e)
+    z = 0.5 * np.ones_like(x)
+    sides = [(x, y, z), (y, x, -z), (y, z, x), (x, -z, y), (z, x, y), (-z, y, x)]
+    parts = [Particle(np.column_stack(s), faces) for s in sides]
+    p = parts[0].vertcat(*parts[1:]).clean()
+    X, Y, Z = p.verts2[:, 0], p.verts2[:, 1], p.verts2[:, 2]
+    az = np.arctan2(Y, X)
+    el = np.arctan2(Z, np.sqrt(X ** 2 + Y ** 2))
+
+    def spow_sin(a):
+        return np.sign(np.sin(a)) * np.abs(np.sin(a)) ** e
+
+    def spow_cos(a):
+        return np.sign(np.cos(a)) * np.abs(np.cos(a)) ** e
+
+    cube = np.column_stack([0.5 * spow_cos(el) * spow_cos(az), 0.5 * spow_cos(el) * spow_sin(az), 0.5 * spow_sin(el)])
+    out = Particle(cube, p.faces2, **kwargs)
+    return out.scale(length)
 
 
 # ---------------------------------------------------------------------------

@@ -6,7 +6,8 @@
     python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1]
     python -m mnpbem_b200.microbench hmat  [--faces 1444] [--cleaf 200] [--htol 1e-6] [--reps 3]
     python -m mnpbem_b200.microbench iter  [--faces 1444] [--hmatrix] [--noprecond] [--tol 1e-10]
-    python -m mnpbem_b200.microbench large [--side 3] [--hmatrix] [--tol 1e-8]
+    python -m mnpbem_b200.microbench large [--side 3 | --shape cube] [--hmatrix] [--tol 1e-8]
+    python -m mnpbem_b200.microbench sweep [--seed 0] [--nlambda 128] [--workers 2] [--schedule interleave|mesh]
 
 ``step`` runs whole per-wavelength solves (assembly + init + solve) of the
 sphere dimer (two trisphere(faces) spheres, 2 nm gap, water, Drude gold,
@@ -18,6 +19,7 @@ import argparse
 import ctypes
 import json
 import sys
+import time
 
 import numpy as np
 
@@ -209,13 +211,21 @@ def sphere_array(side=3, faces=1444, diameter=40.0, gap=2.0, eps_b=1.0):
 
 
 def case_large(a):
-    """One large solve (3 x 3 gold spheres, 25956 faces, vacuum, 700 nm, x-pol):
-    BEMRetIter with the complex64 tensor-core LU as preconditioner and the
-    FP64 dense (or H-matrix) operator."""
+    """One large solve (3 x 3 gold spheres, 25956 faces, or with --shape cube
+    the rounded gold cube tricube(66, 100 nm, e = 0.25), 25344 curved quads;
+    vacuum, 700 nm, x-pol): BEMRetIter with the complex64 tensor-core LU as
+    preconditioner and the FP64 dense (or H-matrix) operator."""
     import torch
     from . import PlaneWaveRet
     from .bem_iter import BEMRetIter
-    cp = sphere_array(a.side)
+    if a.shape == "cube":
+        from . import ComParticle, EpsConst, EpsDrude
+        from .geometry import tricube
+        cp = ComParticle([EpsConst(1.0), EpsDrude(9.84, 9.0, 0.067)], [tricube(a.cube_n, 100.0, a.cube_e,
+                                                                                 interp="curv")],
+                         [[2, 1]], 1, interp="curv")
+    else:
+        cp = sphere_array(a.side)
     exc = PlaneWaveRet(np.array([[1.0, 0, 0]]), np.array([[0, 0, 1.0]]))
     e0, e1, e2 = _events() + (torch.cuda.Event(enable_timing=True),)
     torch.cuda.synchronize()
@@ -226,7 +236,7 @@ def case_large(a):
     sig, _ = bem.solve(exc.potential(cp, 700.0))
     e2.record()
     torch.cuda.synchronize()
-    out = {"case": "large", "faces": cp.n, "hmatrix": a.hmatrix, "tol": a.tol, "ext": exc.extinction(sig),
+    out = {"case": "large", "shape": a.shape, "faces": cp.n, "hmatrix": a.hmatrix, "tol": a.tol, "ext": exc.extinction(sig),
            "sca": exc.scattering(sig)[0], "iters": bem.last.iter, "relres": bem.last.relres,
            "ms_ctor_init": e0.elapsed_time(e1), "ms_solve": e1.elapsed_time(e2),
            "max_mem_GB": torch.cuda.max_memory_allocated() / 1e9}
@@ -235,9 +245,48 @@ def case_large(a):
     return out
 
 
+def case_sweep(a):
+    """The uneven batch: 8 seeded spheres / ellipsoids / rods of 284 ... 5768
+    faces (gold or silver, vacuum), nlambda wavelengths 450-900 nm, x and y
+    polarisations along +z, complex64 factors + FP64 refinement, the (mesh,
+    wavelength) work spread over ``workers`` streams.  ``check`` wavelengths per mesh are re-solved with
+    the fp64 path and the largest extinction error is reported."""
+    import torch
+    from .bem import BEMRet
+    from .planewave import PlaneWaveRet
+    from .sweep import solve_sweep, uneven_meshes
+    pol = np.array([[1.0, 0, 0], [0, 1.0, 0]])
+    dirs = np.array([[0, 0, 1.0], [0, 0, 1.0]])
+    enei = np.linspace(450.0, 900.0, a.nlambda)
+    t0 = time.perf_counter()
+    meshes = uneven_meshes(a.seed)
+    mesh_s = time.perf_counter() - t0
+    r = solve_sweep([m["p"] for m in meshes], enei, pol, dirs, precision=a.precision, workers=a.workers,
+                    schedule=a.schedule)
+    worst = 0.0
+    rng = np.random.default_rng(a.seed + 1)
+    exc = PlaneWaveRet(pol, dirs)
+    for mi, m in enumerate(meshes):
+        ref = BEMRet(m["p"])
+        for i in rng.choice(len(enei), size=min(a.check, len(enei)), replace=False):
+            e64 = ref.cross_sections(exc, float(enei[i]))["ext"]
+            worst = max(worst, float(np.max(np.abs(r["ext"][mi, i] - e64) / np.abs(e64))))
+        del ref
+    torch.cuda.synchronize()
+    return {"case": "sweep", "seed": a.seed, "faces": [m["n"] for m in meshes],
+            "shapes": [m["shape"] for m in meshes], "metals": [m["metal"] for m in meshes],
+            "nlambda": a.nlambda, "npol": 2, "workers": a.workers, "schedule": a.schedule,
+            "precision": a.precision,
+            "solves": r["solves"], "sweep_s": r["sweep_s"], "solves_per_s": r["solves_per_s"],
+            "setup_s": r["setup_s"], "mesh_build_s": mesh_s,
+            "e2e_solves_per_s": r["solves"] / (r["sweep_s"] + r["setup_s"] + mesh_s),
+            "per_worker_s": [round(v, 3) for v in r["per_worker_s"]], "max_ext_relerr_vs_fp64": worst,
+            "max_mem_GB": torch.cuda.max_memory_allocated() / 1e9}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter", "large"])
+    ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter", "large", "sweep"])
     ap.add_argument("--faces", type=int, default=1444)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--engine", type=int, default=1)
@@ -255,6 +304,14 @@ def main(argv=None):
     ap.add_argument("--hmatrix", action="store_true")
     ap.add_argument("--noprecond", action="store_true")
     ap.add_argument("--side", type=int, default=3)
+    ap.add_argument("--shape", default="spheres", choices=["spheres", "cube"])
+    ap.add_argument("--cube-n", dest="cube_n", type=int, default=66)
+    ap.add_argument("--cube-e", dest="cube_e", type=float, default=0.25)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--nlambda", type=int, default=128)
+    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--schedule", default="interleave", choices=["interleave", "mesh"])
+    ap.add_argument("--check", type=int, default=1)
     a = ap.parse_args(argv)
     import torch
     if not torch.cuda.is_available():
@@ -262,7 +319,7 @@ def main(argv=None):
     if a.case == "step":
         a.engine = {0: "simt", 1: "bf16x3", 2: "tf32"}[a.engine]
     out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf, "hmat": case_hmat,
-           "iter": case_iter, "large": case_large}[a.case](a)
+           "iter": case_iter, "large": case_large, "sweep": case_sweep}[a.case](a)
     print(json.dumps(out), flush=True)
 
 

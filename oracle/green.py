@@ -50,8 +50,9 @@ def refine_diag(p1, p2, rows, cols, order=5):
     if nd == 0:
         return g, f
     pos, w, row = p2.quadpol(cols)
-    npts = len(w) // nd
-    if npts * nd != len(w):
+    counts = np.bincount(row, minlength=nd)
+    npts = int(counts[0])
+    if np.any(counts != npts):
         # mixed triangle / quad faces: integrate face by face
         for k in range(nd):
             sel = row == k

@@ -23,8 +23,10 @@ input/output vectors that pin the oracle and the geometry module:
                           checksums of sig (slow: ~1 min).
 * ``hmat_trees.npz``    : reference cluster trees, admissibility block lists and
                           ACA ranks / errors for the sphere and the small dimer.
+* ``meshes.npz``        : face arrays of the reference mesh generators; ext / sca of a
+                          small curved rod, rounded cube and flat ellipsoid.
 
-Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only]
+Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only] [--meshes-only]
 """
 import os
 import sys
@@ -196,10 +198,78 @@ def hmat_trees():
     save("hmat_trees.npz", **out)
 
 
+MESH_CASES = (
+    # tag, generator, args, kwargs, store every face (else a sample)
+    ("ell", "triellipsoid", (400, [10.0, 15.0, 25.0]), {}, True),
+    ("seg", "trispheresegment", (np.linspace(0, np.pi, 7), np.linspace(0, np.pi / 2, 5), 10.0),
+     {"triangles": True, "interp": "curv"}, True),
+    ("rod", "trirod", (20.0, 60.0, [13, 6, 9]), {"interp": "curv"}, True),
+    ("rodtri", "trirod", (12.0, 30.0, [9, 5, 5]), {"triangles": True, "interp": "curv"}, True),
+    ("cube", "tricube", (6, 40.0, 0.25), {"interp": "curv"}, True),
+    ("rod2400", "trirod", (20.0, 80.0, [41, 16, 31]), {"interp": "curv"}, False),
+    ("cube25k", "tricube", (66, 100.0, 0.25), {"interp": "curv"}, False),
+)
+
+
+def _face_nodes(p):
+    """Per-face node coordinates (n, 9, 3), NaN where a face has no such node."""
+    if p.faces2 is None:
+        f, v = p.faces, p.verts
+    else:
+        f, v = p.faces2, p.verts2
+    out = np.full((len(f), 9, 3), np.nan)
+    ok = ~np.isnan(f)
+    out[:, :f.shape[1]][ok] = v[f[ok].astype(int)]
+    return out
+
+
+def meshes():
+    """Face arrays of the reference mesh generators (triellipsoid, trispheresegment,
+    trirod, tricube), and ext / sca of a small curved rod, a rounded cube and a
+    flat ellipsoid (water, Drude gold; x-pol along +z and z-pol along +x) from
+    the reference BEMRet."""
+    from mnpbem.geometry import mesh_generators as mg
+    out = {}
+    for tag, name, args, kw, full in MESH_CASES:
+        p = getattr(mg, name)(*args, **kw)
+        ind = np.arange(p.nfaces) if full else np.arange(0, p.nfaces, max(1, p.nfaces // 40))
+        out[tag + "_nfaces"] = p.nfaces
+        out[tag + "_nverts"] = p.nverts
+        out[tag + "_ntri"] = int(np.sum(np.isnan(p.faces[:, 3])))
+        out[tag + "_ind"] = ind
+        for a in ("pos", "nvec", "tvec1", "area"):
+            out[tag + "_" + a] = getattr(p, a)[ind]
+        out[tag + "_bradius"] = p.bradius()[ind]
+        out[tag + "_nodes"] = _face_nodes(p)[ind]
+        out[tag + "_area_sum"] = np.sum(p.area)
+        out[tag + "_pos_sum"] = np.sum(p.pos, axis=0)
+    for tag, name, args, interp in (("rodbem", "trirod", (12.0, 30.0, [9, 5, 5]), "curv"),
+                                    ("cubebem", "tricube", (5, 20.0, 0.25), "curv"),
+                                    ("ellbem", "triellipsoid", (60, [4.0, 6.0, 9.0]), "flat")):
+        part = getattr(mg, name)(*args) if interp == "flat" else getattr(mg, name)(*args, interp=interp)
+        p = ComParticle([EpsConst(1.77), EpsDrude(*DRUDE_AU)], [part], [[2, 1]], 1, interp=interp)
+        bem = BEMRet(p)
+        exc = PlaneWaveRet(np.array([[1.0, 0, 0], [0, 0, 1.0]]), np.array([[0, 0, 1.0], [1.0, 0, 0]]))
+        enei = np.array([560.0, 640.0])
+        ext, sca = [], []
+        for e in enei:
+            sig, bem = bem.solve(exc.potential(p, e))
+            ext.append(exc.extinction(sig))
+            sca.append(exc.scattering(sig)[0])
+        out[tag + "_enei"], out[tag + "_ext"], out[tag + "_sca"] = enei, np.array(ext), np.array(sca)
+        out[tag + "_nfaces"] = p.nfaces
+        out[tag + "_sig2"] = sig.sig2
+    save("meshes.npz", **out)
+
+
 if __name__ == "__main__":
+    if "--meshes-only" in sys.argv:
+        meshes()
+        sys.exit(0)
     hmat_trees()
     if "--hmat-only" in sys.argv:
         sys.exit(0)
+    meshes()
     geom()
     refined_cfg0()
     matrices_s60()

@@ -25,3 +25,40 @@ def rel(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+# Reference mesh-generator cases pinned by tests/golden/meshes.npz:
+# tag -> (generator, args, kwargs)
+MESH_CASES = {
+    "ell": ("triellipsoid", (400, [10.0, 15.0, 25.0]), {}),
+    "seg": ("trispheresegment", (np.linspace(0, np.pi, 7), np.linspace(0, np.pi / 2, 5), 10.0),
+            {"triangles": True, "interp": "curv"}),
+    "rod": ("trirod", (20.0, 60.0, [13, 6, 9]), {"interp": "curv"}),
+    "rodtri": ("trirod", (12.0, 30.0, [9, 5, 5]), {"triangles": True, "interp": "curv"}),
+    "cube": ("tricube", (6, 40.0, 0.25), {"interp": "curv"}),
+    "rod2400": ("trirod", (20.0, 80.0, [41, 16, 31]), {"interp": "curv"}),
+    "cube25k": ("tricube", (66, 100.0, 0.25), {"interp": "curv"}),
+}
+
+
+def shape_particle(tag, eps_b=1.77, drude=DRUDE_AU):
+    """ComParticle of one reference-generator case in a medium eps_b.
+    'rodbem' = trirod(12, 30, [9, 5, 5]) and 'cubebem' = tricube(5, 20, 0.25),
+    both curved, and 'ellbem' = triellipsoid(60, [4, 6, 9]), flat, are the
+    meshes whose BEM results the fixtures hold."""
+    from mnpbem_b200 import geometry
+    extra = {"rodbem": ("trirod", (12.0, 30.0, [9, 5, 5]), {"interp": "curv"}),
+             "cubebem": ("tricube", (5, 20.0, 0.25), {"interp": "curv"}),
+             "ellbem": ("triellipsoid", (60, [4.0, 6.0, 9.0]), {})}
+    name, args, kw = extra[tag] if tag in extra else MESH_CASES[tag]
+    part = getattr(geometry, name)(*args, **kw)
+    return ComParticle([EpsConst(eps_b), EpsDrude(*drude)], [part], [[2, 1]], 1, interp=kw.get("interp", "flat"))
+
+
+def face_nodes(p):
+    """Per-face node coordinates (n, 9, 3), NaN where a face has no such node."""
+    f, v = (p.faces, p.verts) if p.faces2 is None else (p.faces2, p.verts2)
+    out = np.full((len(f), 9, 3), np.nan)
+    ok = ~np.isnan(f)
+    out[:, :f.shape[1]][ok] = v[f[ok].astype(int)]
+    return out
