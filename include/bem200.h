@@ -7,7 +7,9 @@
  * (BEM200_OK = 0).  On failure the message is kept per host thread and read
  * with bem200_last_error().  The caller owns all memory; functions that need
  * scratch space take a workspace pointer whose size is given by the matching
- * *_workspace_size query.  No entry point keeps global mutable state.
+ * *_workspace_size query.  No entry point keeps global mutable state, with
+ * one exception: bem200_getrs_noalloc works in a fixed device buffer that the
+ * library owns (see its declaration).
  *
  * Matrices are dense, row-major, complex (interleaved re/im), with leading
  * dimension `ld` in elements.  Face arrays are (n, 3) row-major float64.

@@ -7,7 +7,8 @@
     python -m mnpbem_b200.microbench hmat  [--faces 1444] [--cleaf 200] [--htol 1e-6] [--reps 3]
     python -m mnpbem_b200.microbench iter  [--faces 1444] [--hmatrix] [--noprecond] [--tol 1e-10]
     python -m mnpbem_b200.microbench large [--side 3 | --shape cube] [--hmatrix] [--tol 1e-8]
-    python -m mnpbem_b200.microbench sweep [--seed 0] [--nlambda 128] [--workers 2] [--schedule interleave|mesh]
+    python -m mnpbem_b200.microbench sweep [--seed 0] [--nlambda 128] [--workers 4] [--schedule interleave|mesh]
+    python -m mnpbem_b200.microbench shape [--nlambda 5] [--ndir 32] [--check 4] [--precision mixed]
 
 ``step`` runs whole per-wavelength solves (assembly + init + solve) of the
 sphere dimer (two trisphere(faces) spheres, 2 nm gap, water, Drude gold,
@@ -284,9 +285,61 @@ def case_sweep(a):
             "max_mem_GB": torch.cuda.max_memory_allocated() / 1e9}
 
 
+def case_shape(a):
+    """Gradients of the extinction of the gold rod trirod(20, 80, [41, 16, 31])
+    (2400 curved faces, eps_b 1.77, x-pol along +z) at nlambda wavelengths
+    600-800 nm: 32 seeded vertex directions (ShapeSensitivity) and the
+    permittivity gradient; ``check`` directions at the middle wavelength are
+    compared with central differences of full fp64 solves (step 1e-4 nm)."""
+    import torch
+    from . import BEMRet, ComParticle, EpsConst, EpsDrude, PlaneWaveRet
+    from .adjoint import extinction_eps_gradient
+    from .geometry import trirod
+    from .shape import ShapeSensitivity, perturbed, random_directions
+    cp = ComParticle([EpsConst(1.77), EpsDrude(9.84, 9.0, 0.067)], [trirod(20.0, 80.0, [41, 16, 31],
+                                                                             interp="curv")],
+                     [[2, 1]], 1, interp="curv")
+    exc = PlaneWaveRet(np.array([[1.0, 0, 0]]), np.array([[0, 0, 1.0]]))
+    D = random_directions(cp, a.ndir, seed=a.seed)
+    enei = np.linspace(600.0, 800.0, a.nlambda)
+    bem = BEMRet(cp, precision=a.precision)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sens = ShapeSensitivity(bem, D, 1e-4)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    exts, dexts, t_lam, t_eps = [], [], [], []
+    for e in enei:
+        t1 = time.perf_counter()
+        ext, dext = sens.extinction(exc, float(e))
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        _, geps = extinction_eps_gradient(bem, exc, float(e), 2)
+        torch.cuda.synchronize()
+        t_lam.append(t2 - t1)
+        t_eps.append(time.perf_counter() - t2)
+        exts.append(float(ext[0]))
+        dexts.append(dext[:, 0])
+    mid = len(enei) // 2
+    worst = 0.0
+    for k in range(min(a.check, a.ndir)):
+        e2 = []
+        for s in (1.0, -1.0):
+            q = perturbed(cp, s * 1e-4 * D[k])
+            sig, _ = BEMRet(q).solve(exc.potential(q, float(enei[mid])))
+            e2.append(float(exc.extinction(sig)))
+        fd = (e2[0] - e2[1]) / 2e-4
+        worst = max(worst, abs(dexts[mid][k] - fd) / np.max(np.abs(dexts[mid])))
+    return {"case": "shape", "faces": cp.n, "nvert": int(D.shape[1]), "ndir": a.ndir, "nlambda": a.nlambda,
+            "precision": a.precision, "ext": exts, "setup_s": t_setup, "s_per_lambda_32dir": t_lam,
+            "s_per_lambda_eps_grad": t_eps, "max_fd_relerr": worst, "fd_checked": min(a.check, a.ndir),
+            "max_mem_GB": torch.cuda.max_memory_allocated() / 1e9}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter", "large", "sweep"])
+    ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter", "large", "sweep",
+                                           "shape"])
     ap.add_argument("--faces", type=int, default=1444)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--engine", type=int, default=1)
@@ -309,9 +362,10 @@ def main(argv=None):
     ap.add_argument("--cube-e", dest="cube_e", type=float, default=0.25)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--nlambda", type=int, default=128)
-    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--schedule", default="interleave", choices=["interleave", "mesh"])
     ap.add_argument("--check", type=int, default=1)
+    ap.add_argument("--ndir", type=int, default=32)
     a = ap.parse_args(argv)
     import torch
     if not torch.cuda.is_available():
@@ -319,7 +373,8 @@ def main(argv=None):
     if a.case == "step":
         a.engine = {0: "simt", 1: "bf16x3", 2: "tf32"}[a.engine]
     out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf, "hmat": case_hmat,
-           "iter": case_iter, "large": case_large, "sweep": case_sweep}[a.case](a)
+           "iter": case_iter, "large": case_large, "sweep": case_sweep,
+           "shape": case_shape}[a.case](a)
     print(json.dumps(out), flush=True)
 
 

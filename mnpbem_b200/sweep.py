@@ -109,7 +109,7 @@ def sweep_plan(sizes, nlambda, workers, schedule="interleave"):
     return plan
 
 
-def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=2, engine="bf16x3", schedule="interleave",
+def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=4, engine="bf16x3", schedule="interleave",
                 **bem_kwargs):
     """Extinction and scattering of every particle at every wavelength.
 
