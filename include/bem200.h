@@ -293,6 +293,26 @@ int bem200_hmat_matvec(int n, int w, const void* x, int nl, const int32_t* lblk,
                        const void* U, const void* V, void* T, int nd, const int32_t* dblk, const int64_t* doff,
                        const void* D, void* y, void* stream);
 
+/* bem200_hmat_compress_green: the dense leaves and the ACA of the low-rank
+ * blocks of BEM matrix `which` (0 = G1, 1 = G2, 2 = H1, 3 = H2) with every
+ * entry computed on demand from the Green function, so no n x n matrix is
+ * stored: rows and columns of a block come from the face arrays (pos, nvec,
+ * area), the region table (pid, blk_mat, kmat as in bem200_green_assemble)
+ * and the refinement tables in CSR form (ref_row_ptr (n + 1) int64, ref_col,
+ * g, fn; ref_row_ptr NULL = no refined pairs).  Block indices are in cluster
+ * order; c2p maps them to faces.  Entries equal those of
+ * bem200_green_assemble; the ACA is that of bem200_hmat_aca.  Replaces the
+ * reference's densify-then-compress fill (ACACompGreenRet,
+ * mnpbem/greenfun/aca_compgreen_ret.py:184-208) with the on-demand rows and
+ * columns of the MEX library (mex/acagreen/acagreen.cpp:83-149). */
+int bem200_hmat_compress_green(int which, int n, int npart, const int32_t* pid, const int32_t* blk_mat, int nmat,
+                               const double* kmat_host, const double* pos, const double* nvec, const double* area,
+                               const int64_t* ref_row_ptr, const int32_t* ref_col, int order, const double* g,
+                               const double* fn, const int32_t* c2p, int nd, const int32_t* dblk,
+                               const int64_t* doff, void* D, int nl, const int32_t* lblk, const int64_t* uoff,
+                               const int64_t* voff, const int32_t* kcap, double htol, void* U, void* V,
+                               int32_t* rank, int max_rows, int max_kcap, void* stream);
+
 /* ------------------------------------------------------------- Krylov
  * Kernels of the restarted GMRES of the iterative solver (complex128), which
  * replaces scipy.sparse.linalg.gmres as driven by BEMIter._iter_solve

@@ -81,6 +81,10 @@ _SIGS = {
                                        ctypes.c_int, ctypes.c_int, _vp]),
     "bem200_hmat_matvec": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
                                           _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "bem200_hmat_compress_green": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int,
+                                                  _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp,
+                                                  ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                                  _dbl, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "bem200_planewave_rhs": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _dbl,
                                             ctypes.c_int, _vp, _vp, _vp, _vp]),
     "bem200_farfield": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _dbl, _vp,

@@ -100,6 +100,21 @@ class BEMRet:
         n = self.n = p.n
         prec = 0 if precision == "fp64" else 1
         self._prec = prec
+        self._ws = None      # factor workspaces, allocated by the first init()
+        self._nvec = torch.as_tensor(np.ascontiguousarray(p.nvec), dtype=torch.float64, device=self.dev)
+        self.last_ir = None
+        if enei is not None:
+            self.init(enei)
+
+    def _alloc(self):
+        """Workspaces of the factors: 7 n x n slots, the GEMM operand space and,
+        for the mixed path, the complex128 matrices of the FP64 operator.  Users
+        that never factor (the unpreconditioned iterative solver) never pay for
+        them."""
+        if self._ws is not None:
+            return
+        torch = _torch()
+        n, prec = self.n, self._prec
         L = nat.lib()
         self._ws = torch.empty(int(L.bem200_bem_workspace_size(prec, n)), dtype=torch.uint8, device=self.dev)
         slots = [ctypes.c_void_p() for _ in range(4)]
@@ -110,12 +125,8 @@ class BEMRet:
         gbytes = int(L.bem200_gemm_workspace_size(_ENGINES[self.engine], n, n, n) * 5 // 4)
         self._gws = torch.empty(max(gbytes, 1), dtype=torch.uint8, device=self.dev)
         self._gws_bytes = gbytes
-        self._nvec = torch.as_tensor(np.ascontiguousarray(p.nvec), dtype=torch.float64, device=self.dev)
         if prec == 1:
             self._G128 = [torch.empty((n, n), dtype=torch.complex128, device=self.dev) for _ in range(4)]
-        self.last_ir = None
-        if enei is not None:
-            self.init(enei)
 
     # ----------------------------------------------------------------- eps
     def _eps(self, enei):
@@ -141,6 +152,7 @@ class BEMRet:
         (reference bem_ret.py:293-525).  Skipped if already initialised there."""
         if self.enei is not None and np.isclose(self.enei, enei):
             return self
+        self._alloc()
         n = self.n
         self.k = 2 * np.pi / enei
         self._eps(enei)

@@ -155,7 +155,10 @@ class BEMRetIter:
     restart=None (= maxit), precond='hmat' (dense BEM factors as M) or None,
     output=0; hmatrix=False (True: H-matrix operator, htol=1e-6,
     kmax=[4, 100], cleaf=200, eta=2.5); B200 options: precond_precision
-    ('mixed' | 'fp64'), engine ('bf16x3' | 'simt').
+    ('mixed' | 'fp64'), engine ('bf16x3' | 'simt'), hmat_fill ('auto':
+    compress the dense matrices the mixed preconditioner keeps, otherwise
+    compute every stored H-matrix entry on demand from the Green function;
+    'green' | 'dense' force one way).
     """
 
     name = "bemsolver"
@@ -163,7 +166,7 @@ class BEMRetIter:
 
     def __init__(self, p, enei=None, solver="gmres", tol=1e-4, maxit=200, restart=None, precond="hmat", output=0,
                  hmatrix=False, htol=1e-6, kmax=(4, 100), cleaf=200, eta=2.5, precond_precision="mixed",
-                 engine="bf16x3", **options):
+                 engine="bf16x3", hmat_fill="auto", **options):
         torch = _torch()
         if p is None:
             raise ValueError("BEMRetIter: 'p' must be a ComParticle (or compatible particle object), got None.")
@@ -176,9 +179,12 @@ class BEMRetIter:
             raise ValueError("[error] iterative solver not known: <{}>".format(solver))
         if precond not in ("hmat", None):
             raise ValueError("BEMRetIter: precond must be 'hmat' or None")
+        if hmat_fill not in ("auto", "green", "dense"):
+            raise ValueError("BEMRetIter: hmat_fill must be 'auto', 'green' or 'dense'")
         if not torch.cuda.is_available():
             raise RuntimeError("BEMRetIter: a CUDA device is required (no CPU fallback)")
         self.p = p
+        self.hmat_fill = hmat_fill
         self.solver = solver
         self.tol = float(tol)
         self.maxit = int(maxit)
@@ -226,8 +232,11 @@ class BEMRetIter:
             if self._hmat is None:
                 self._hmat = BEMHMatrices(self.p, self.g, htol=self.htol, kmax=self.kmax, cleaf=self.cleaf,
                                           eta=self.eta)
-            shared = bem._G128 if (self.precond is not None and bem._prec == 1) else None
-            self._hmat.build(enei, mats=shared)
+            # 'auto': reuse the dense matrices the mixed preconditioner keeps, else
+            # compute the stored entries on demand; 'green' / 'dense' force one way
+            have = self.precond is not None and bem._prec == 1
+            shared = bem._G128 if (have and self.hmat_fill != "green") else None
+            self._hmat.build(enei, mats=shared, fill="dense" if self.hmat_fill == "dense" else "green")
         else:
             if bem._prec == 1 and self.precond is not None:
                 self._G = bem._G128  # assembled by the mixed init

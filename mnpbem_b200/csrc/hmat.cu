@@ -13,10 +13,18 @@
 #include <cfloat>
 
 #include "common.cuh"
+#include "green_entry.cuh"
 
 namespace bem200 {
 
 constexpr int kHThreads = 256;
+
+// Entry (ci, cj) of a dense n x n matrix already in cluster order.
+struct DenseSource {
+  const double2* Mc;
+  int n;
+  __device__ __forceinline__ double2 operator()(int ci, int cj) const { return Mc[(long long)ci * n + cj]; }
+};
 
 __device__ __forceinline__ double cmod(double2 a) { return hypot(a.x, a.y); }
 
@@ -38,14 +46,15 @@ __global__ void permute_kernel(int n, const double2* __restrict__ src, const int
   for (int j = threadIdx.x; j < n; j += blockDim.x) drow[j] = srow[c2p[j]];
 }
 
-__global__ void pack_dense_kernel(const int32_t* __restrict__ blk, const int64_t* __restrict__ off, int n,
-                                  const double2* __restrict__ Mc, double2* __restrict__ D) {
+template <typename Src>
+__global__ void pack_dense_kernel(const int32_t* __restrict__ blk, const int64_t* __restrict__ off, Src src,
+                                  double2* __restrict__ D) {
   const int b = blockIdx.x;
   const int r0 = blk[4 * b], m = blk[4 * b + 1], c0 = blk[4 * b + 2], nb = blk[4 * b + 3];
   double2* out = D + off[b];
   for (long long e = threadIdx.x; e < (long long)m * nb; e += blockDim.x) {
     const int i = (int)(e / nb), j = (int)(e % nb);
-    out[e] = Mc[(long long)(r0 + i) * n + c0 + j];
+    out[e] = src(r0 + i, c0 + j);
   }
 }
 
@@ -104,9 +113,11 @@ __device__ double block_sum_d(double v, double* sv) {
 // Partially pivoted ACA of one admissible block per CTA.  Shared memory:
 // used-row / used-column flags (m + nb bytes), U[p, :k] and V[pc, :k]
 // (kcap complex each), the per-l partial cross dots (2 x kcap complex).
+// The block's entries come from `src`: a stored matrix or the Green function.
+template <typename Src>
 __global__ void __launch_bounds__(kHThreads) aca_kernel(const int32_t* __restrict__ blk, const int64_t* __restrict__ uoff,
                                                        const int64_t* __restrict__ voff, const int32_t* __restrict__ kcap_arr,
-                                                       int n, const double2* __restrict__ Mc, double htol,
+                                                       Src src, double htol,
                                                        double2* __restrict__ Ug, double2* __restrict__ Vg,
                                                        int32_t* __restrict__ rank_out) {
   extern __shared__ __align__(16) unsigned char aca_smem[];
@@ -137,9 +148,8 @@ __global__ void __launch_bounds__(kHThreads) aca_kernel(const int32_t* __restric
     double best = -1.0;
     int bj = INT_MAX;
     double vsq = 0.0;
-    const double2* mrow = Mc + (long long)(r0 + p) * n + c0;
     for (int j = tid; j < nb; j += kHThreads) {
-      double2 val = mrow[j];
+      double2 val = src(r0 + p, c0 + j);
       const double2* vj = V + (long long)j * kc;
       for (int l = 0; l < k; ++l) val = csub(val, cmul(Up[l], vj[l]));
       V[(long long)j * kc + k] = val;
@@ -166,7 +176,7 @@ __global__ void __launch_bounds__(kHThreads) aca_kernel(const int32_t* __restric
     best = -1.0;
     int bi = INT_MAX;
     for (int i = tid; i < m; i += kHThreads) {
-      double2 val = Mc[(long long)(r0 + i) * n + c0 + pc];
+      double2 val = src(r0 + i, c0 + pc);
       const double2* ui = U + (long long)i * kc;
       for (int l = 0; l < k; ++l) val = csub(val, cmul(ui[l], Vp[l]));
       const double2 u = cdiv(val, pv);
@@ -343,7 +353,8 @@ int bem200_hmat_pack_dense(int nd, const int32_t* dblk, const int64_t* doff, int
   BEM_REQUIRE(nd >= 0 && n > 0, BEM200_ERR_ARG, "hmat_pack_dense: bad sizes");
   if (nd == 0) return BEM200_OK;
   BEM_REQUIRE(dblk && doff && Mc && D, BEM200_ERR_ARG, "hmat_pack_dense: null pointer");
-  pack_dense_kernel<<<nd, 256, 0, (cudaStream_t)stream>>>(dblk, doff, n, (const double2*)Mc, (double2*)D);
+  pack_dense_kernel<DenseSource><<<nd, 256, 0, (cudaStream_t)stream>>>(dblk, doff, DenseSource{(const double2*)Mc, n},
+                                                                        (double2*)D);
   BEM_LAUNCH_CHECK();
   return BEM200_OK;
 }
@@ -358,10 +369,62 @@ int bem200_hmat_aca(int nl, const int32_t* lblk, const int64_t* uoff, const int6
   const size_t smem = (size_t)4 * max_kcap * sizeof(double2) + 2 * (size_t)max_rows + 16;
   BEM_REQUIRE(smem <= 200 * 1024, BEM200_ERR_UNSUPPORTED, "hmat_aca: block of %d rows / rank %d too large", max_rows,
               max_kcap);
-  BEM_CUDA_CHECK(set_kernel_attrs_once(aca_kernel, (int)smem, false));
-  aca_kernel<<<nl, kHThreads, smem, (cudaStream_t)stream>>>(lblk, uoff, voff, kcap, n, (const double2*)Mc, htol,
-                                                           (double2*)U, (double2*)V, rank);
+  BEM_CUDA_CHECK(set_kernel_attrs_once(aca_kernel<DenseSource>, (int)smem, false));
+  aca_kernel<DenseSource><<<nl, kHThreads, smem, (cudaStream_t)stream>>>(
+      lblk, uoff, voff, kcap, DenseSource{(const double2*)Mc, n}, htol, (double2*)U, (double2*)V, rank);
   BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+int bem200_hmat_compress_green(int which, int n, int npart, const int32_t* pid, const int32_t* blk_mat, int nmat,
+                               const double* kmat_host, const double* pos, const double* nvec, const double* area,
+                               const int64_t* ref_row_ptr, const int32_t* ref_col, int order, const double* g,
+                               const double* fn, const int32_t* c2p, int nd, const int32_t* dblk,
+                               const int64_t* doff, void* D, int nl, const int32_t* lblk, const int64_t* uoff,
+                               const int64_t* voff, const int32_t* kcap, double htol, void* U, void* V,
+                               int32_t* rank, int max_rows, int max_kcap, void* stream) {
+  BEM_REQUIRE(which >= 0 && which <= 3 && n > 0 && npart > 0 && nmat > 0 && nmat <= ge::kMaxMat && kmat_host &&
+                  pid && blk_mat && pos && nvec && area && c2p && order >= 0 && order <= ge::kMaxOrder &&
+                  nd >= 0 && nl >= 0 && htol >= 0,
+              BEM200_ERR_ARG, "hmat_compress_green: bad arguments");
+  BEM_REQUIRE(ref_row_ptr ? (ref_col && g && fn) : true, BEM200_ERR_ARG,
+              "hmat_compress_green: refinement tables incomplete");
+  ge::GreenSource src;
+  src.n = n;
+  src.npart = npart;
+  src.which = which;
+  src.order = order;
+  src.pid = pid;
+  src.blk_mat = blk_mat;
+  src.pos = pos;
+  src.nvec = nvec;
+  src.area = area;
+  src.row_ptr = ref_row_ptr;
+  src.ref_col = ref_col;
+  src.g = g;
+  src.fn = fn;
+  src.c2p = c2p;
+  for (int m = 0; m < ge::kMaxMat; ++m) {
+    src.kre[m] = m < nmat ? kmat_host[2 * m] : 0.0;
+    src.kim[m] = m < nmat ? kmat_host[2 * m + 1] : 0.0;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  if (nd > 0) {
+    BEM_REQUIRE(dblk && doff && D, BEM200_ERR_ARG, "hmat_compress_green: null dense-leaf pointer");
+    pack_dense_kernel<ge::GreenSource><<<nd, 256, 0, s>>>(dblk, doff, src, (double2*)D);
+    BEM_LAUNCH_CHECK();
+  }
+  if (nl > 0) {
+    BEM_REQUIRE(lblk && uoff && voff && kcap && U && V && rank, BEM200_ERR_ARG,
+                "hmat_compress_green: null low-rank pointer");
+    const size_t smem = (size_t)4 * max_kcap * sizeof(double2) + 2 * (size_t)max_rows + 16;
+    BEM_REQUIRE(smem <= 200 * 1024, BEM200_ERR_UNSUPPORTED, "hmat_compress_green: block of %d rows / rank %d too large",
+                max_rows, max_kcap);
+    BEM_CUDA_CHECK(set_kernel_attrs_once(aca_kernel<ge::GreenSource>, (int)smem, false));
+    aca_kernel<ge::GreenSource><<<nl, kHThreads, smem, s>>>(lblk, uoff, voff, kcap, src, htol, (double2*)U,
+                                                             (double2*)V, rank);
+    BEM_LAUNCH_CHECK();
+  }
   return BEM200_OK;
 }
 

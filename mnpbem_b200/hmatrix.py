@@ -244,6 +244,28 @@ class HMatrixGPU:
             self.ranks = np.zeros(0, dtype=np.int32)
         return self
 
+    def compress_green(self, g, enei, which):
+        """Compress BEM matrix ``which`` (0 = G1, 1 = G2, 2 = H1, 3 = H2) of the
+        Green function ``g`` (a CompGreenRet) at ``enei`` with every entry of the
+        dense leaves and of the ACA rows and columns computed on demand: no
+        n x n matrix is formed (bem200_hmat_compress_green)."""
+        ks = g.wavenumbers(enei)
+        kmat = (ctypes.c_double * (2 * len(ks)))(*[v for k in ks for v in (k.real, k.imag)])
+        blk = g._blk_mat([(0, 0), (1, 0), (1, 1), (0, 1)])
+        r = g.refined
+        has_ref = r.nref > 0
+        max_rows = int(max(self._lb[:, 1].max(), self._lb[:, 3].max())) if self.nlow else 1
+        max_kcap = int(self._kcap.max()) if self.nlow else 1
+        nat.call("bem200_hmat_compress_green", int(which), self.n, g.npart, nat.ptr(g.pid), nat.ptr(blk), len(ks),
+                 ctypes.cast(kmat, ctypes.c_void_p), nat.ptr(g.pos), nat.ptr(g.nvec), nat.ptr(g.area),
+                 nat.ptr(r.row_ptr) if has_ref else None, nat.ptr(r.col) if has_ref else None, g.order,
+                 nat.ptr(r.g) if has_ref else None, nat.ptr(r.fn) if has_ref else None, nat.ptr(self.c2p),
+                 self.ndense, nat.ptr(self.dblk), nat.ptr(self.doff), nat.ptr(self.D), self.nlow, nat.ptr(self.lblk),
+                 nat.ptr(self.uoff), nat.ptr(self.voff), nat.ptr(self.kcap), self.htol, nat.ptr(self.U),
+                 nat.ptr(self.V), nat.ptr(self.rank), max_rows, max_kcap, nat.stream_ptr())
+        self.ranks = self.rank.cpu().numpy()[:self.nlow].copy() if self.nlow else np.zeros(0, dtype=np.int32)
+        return self
+
     def compression(self):
         """Stored elements / n^2 (reference HMatrix.compression, hmatrix.py:739-756)."""
         ne = int(self._doff_h[-1]) + int(np.sum(self.ranks.astype(np.int64) * (self._lb[:, 1] + self._lb[:, 3])))
@@ -273,10 +295,11 @@ def particle_index(p):
 class BEMHMatrices:
     """G1, G2, H1, H2 of the BEM as device H-matrices and the BEM operator on them.
 
-    ``build(enei)`` assembles the dense matrices with the GPU Green kernels,
-    compresses them (wavenumber-aware admissibility at k = 2 pi / enei, as the
-    reference ACACompGreenRet.eval, aca_compgreen_ret.py:156-164) and frees
-    the dense copies; ``apply`` is the FP64 operator of ``bem200_bem_apply``
+    ``build(enei)`` compresses the four matrices (wavenumber-aware
+    admissibility at k = 2 pi / enei, as the reference ACACompGreenRet.eval,
+    aca_compgreen_ret.py:156-164): from dense matrices already at hand, or
+    with entries computed on demand from the Green function (the default when
+    none are given); ``apply`` is the FP64 operator of ``bem200_bem_apply``
     with the four products done by H-matrix matvecs.
     """
 
@@ -292,14 +315,25 @@ class BEMHMatrices:
         self.H = None
         self.enei = None
 
-    def build(self, enei, mats=None):
-        """Compress G1, G2, H1, H2 at ``enei``; ``mats`` may hand in the four
-        dense complex128 matrices already assembled at this wavelength."""
+    def build(self, enei, mats=None, fill="green"):
+        """Compress G1, G2, H1, H2 at ``enei``.  ``mats`` may hand in the four
+        dense complex128 matrices already assembled at this wavelength;
+        without them, fill='green' computes every stored entry on demand from
+        the Green function (no n x n matrix), fill='dense' assembles the dense
+        matrices first."""
         torch = _torch()
         n = self.n
         fad = make_kaware_fadmiss(2.0 * np.pi / enei, eta0=self.eta)
         dense, low = block_partition(self.tree, fad)
         dev = self.g.device
+        if mats is None and fill == "green":
+            self.H = None
+            self.H = [HMatrixGPU(self.tree, dense, low, htol=self.htol, kmax=self.kmax).compress_green(self.g, enei, w)
+                      for w in range(4)]
+            self.enei = enei
+            return self
+        if fill not in ("green", "dense"):
+            raise ValueError("BEMHMatrices.build: fill must be 'green' or 'dense'")
         if mats is None:
             mats = [torch.empty((n, n), dtype=torch.complex128, device=dev) for _ in range(4)]
             self.g.bem_matrices(enei, dtype="c128", out=mats)

@@ -142,16 +142,18 @@ def case_getrf(a):
 
 
 def case_hmat(a):
-    """H-matrix of the dimer's G1: build (dense assembly + ACA of the four
-    BEM matrices), compression and the matvec with 8 right-hand columns."""
+    """H-matrix of the dimer's G1: build of the four BEM matrices (--fill green:
+    dense leaves and ACA rows / columns computed on demand; dense: dense
+    assembly, then ACA), compression and the matvec with 8 right-hand columns."""
     import torch
     from .greenfun import CompGreenRet
     from .hmatrix import BEMHMatrices
     cp = dimer(a.faces)
     g = CompGreenRet(cp, cp)
     hb = BEMHMatrices(cp, g, htol=a.htol, kmax=100, cleaf=a.cleaf, eta=2.5)
-    hb.build(650.0)
-    ms_build = _timed(lambda: hb.build(650.0), 1)
+    fill = "green" if a.fill == "auto" else a.fill
+    hb.build(650.0, fill=fill)
+    ms_build = _timed(lambda: hb.build(650.0, fill=fill), 1)
     h = hb.H[0]
     n, w = cp.n, 8
     gen = torch.Generator(device="cuda").manual_seed(0)
@@ -161,7 +163,8 @@ def case_hmat(a):
     ms_mv = _timed(lambda: h.matvec(x, y, w), a.reps)
     stored = int(h._doff_h[-1]) + int(np.sum(h.ranks.astype(np.int64) * (h._lb[:, 1] + h._lb[:, 3])))
     nbytes = 16 * stored
-    return {"case": "hmat", "faces": n, "cleaf": a.cleaf, "htol": a.htol, "ms_build_4_matrices": ms_build,
+    return {"case": "hmat", "faces": n, "cleaf": a.cleaf, "htol": a.htol, "fill": fill,
+            "ms_build_4_matrices": ms_build,
             "compression": hb.compression(), "dense_blocks": h.ndense, "lowrank_blocks": h.nlow,
             "max_rank": int(h.ranks.max()) if h.nlow else 0, "ms_matvec_w8": ms_mv,
             "matvec_factor_GBps": nbytes / ms_mv / 1e6, "dense_matvec_bytes": 16 * n * n}
@@ -231,13 +234,15 @@ def case_large(a):
     e0, e1, e2 = _events() + (torch.cuda.Event(enable_timing=True),)
     torch.cuda.synchronize()
     e0.record()
-    bem = BEMRetIter(cp, hmatrix=a.hmatrix, cleaf=a.cleaf, htol=a.htol, tol=a.tol)
+    bem = BEMRetIter(cp, hmatrix=a.hmatrix, cleaf=a.cleaf, htol=a.htol, tol=a.tol, hmat_fill=a.fill,
+                     precond=None if a.noprecond else "hmat", maxit=1000)
     bem.init(700.0)
     e1.record()
     sig, _ = bem.solve(exc.potential(cp, 700.0))
     e2.record()
     torch.cuda.synchronize()
-    out = {"case": "large", "shape": a.shape, "faces": cp.n, "hmatrix": a.hmatrix, "tol": a.tol, "ext": exc.extinction(sig),
+    out = {"case": "large", "shape": a.shape, "faces": cp.n, "hmatrix": a.hmatrix, "fill": a.fill,
+           "precond": not a.noprecond, "tol": a.tol, "ext": exc.extinction(sig),
            "sca": exc.scattering(sig)[0], "iters": bem.last.iter, "relres": bem.last.relres,
            "ms_ctor_init": e0.elapsed_time(e1), "ms_solve": e1.elapsed_time(e2),
            "max_mem_GB": torch.cuda.max_memory_allocated() / 1e9}
@@ -366,6 +371,7 @@ def main(argv=None):
     ap.add_argument("--schedule", default="interleave", choices=["interleave", "mesh"])
     ap.add_argument("--check", type=int, default=1)
     ap.add_argument("--ndir", type=int, default=32)
+    ap.add_argument("--fill", default="auto", choices=["auto", "green", "dense"])
     a = ap.parse_args(argv)
     import torch
     if not torch.cuda.is_available():

@@ -135,6 +135,9 @@ def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=4, engine
     t0 = time.perf_counter()
     bems = [{m: BEMRet(particles[m], precision=precision, engine=engine, **bem_kwargs) for m, _ in plan[w]}
             for w in range(workers)]
+    for per in bems:
+        for b in per.values():
+            b._alloc()    # workspaces now, not inside the timed loops
     torch.cuda.synchronize()
     setup = time.perf_counter() - t0
     ext = np.zeros((nm, len(enei), npol))

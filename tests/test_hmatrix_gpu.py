@@ -104,3 +104,47 @@ def test_bem_iter_hmatrix(cuda, mk):
     assert abs(ext - ref["ext"][0]) / abs(ref["ext"][0]) < 1e-5
     comp = bem._hmat.compression()
     assert all(c > 0 for c in comp)
+
+
+@pytest.mark.parametrize("tag", ["s", "d"])
+def test_green_fill_matches_dense_fill(cuda, tag):
+    """bem200_hmat_compress_green (entries on demand, no n x n matrix) against
+    compressing the assembled dense matrices, for G1, G2, H1, H2."""
+    from mnpbem_b200.greenfun import CompGreenRet
+    cp, cleaf, eta = _case(tag)
+    g = CompGreenRet(cp, cp)
+    mats = g.bem_matrices(ENEI, dtype="c128")
+    t = ClusterTree(cp.pos, cleaf=cleaf, ipart_arr=particle_index(cp))
+    dense, low = block_partition(t, make_kaware_fadmiss(2 * np.pi / ENEI, eta0=eta))
+    for which, M in enumerate(mats):
+        hd = HMatrixGPU(t, dense, low, htol=1e-6, kmax=100).compress(M)
+        hg = HMatrixGPU(t, dense, low, htol=1e-6, kmax=100).compress_green(g, ENEI, which)
+        # dense leaves: the same entries as the assembly kernels, to rounding
+        assert rel(hg.D.cpu().numpy(), hd.D.cpu().numpy()) < 1e-13, which
+        assert np.mean(hg.ranks == hd.ranks) > 0.9, which
+        Md = M.cpu().numpy()
+        fg = _reconstruct(hg)
+        assert np.linalg.norm(fg - _reconstruct(hd)) / np.linalg.norm(Md) < 1e-5, which
+        assert np.linalg.norm(fg - Md) / np.linalg.norm(Md) < 1e-5, which
+
+
+def test_bem_iter_hmatrix_green_fill(cuda):
+    """BEMRetIter(hmatrix=True) with the on-demand fill, unpreconditioned and
+    preconditioned, against the fill from the dense matrices."""
+    from mnpbem_b200 import PlaneWaveRet
+    from mnpbem_b200.bem_iter import BEMRetIter
+    cp, cleaf, eta = _case("d")
+    exc = PlaneWaveRet(POL, DIR)
+    ext = {}
+    for fill in ("green", "dense"):
+        for precond in ("hmat", None):
+            bem = BEMRetIter(cp, hmatrix=True, cleaf=cleaf, eta=eta, htol=1e-6, tol=1e-9, maxit=400,
+                             precond=precond, hmat_fill=fill)
+            sig, _ = bem.solve(exc.potential(cp, ENEI))
+            it, rr, fl = bem.info()
+            assert fl[-1] == 0 and rr[-1] <= 1e-9, (fill, precond, it, rr)
+            ext[fill, precond] = exc.extinction(sig)
+    for precond in ("hmat", None):
+        assert abs(ext["green", precond] - ext["dense", precond]) / abs(ext["dense", precond]) < 1e-6
+    ref = OracleBEM(cp).solve(ENEI, POL, DIR)["ext"][0]
+    assert abs(ext["green", None] - ref) / abs(ref) < 1e-5
