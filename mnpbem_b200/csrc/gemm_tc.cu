@@ -31,6 +31,7 @@ constexpr int BM = 128;         // rows of the real output tile
 constexpr int BN = 256;         // real columns of the output tile (128 complex)
 constexpr int BK = 64;          // bf16 per K slab (128 bytes: one swizzle row)
 constexpr int STAGES = 2;
+constexpr int kGroupM = 16;       // tile rows per band of the grouped CTA order
 constexpr int UMMA_K = 16;
 constexpr int A_TILE = BM * BK * 2;   // bytes (16 KB)
 constexpr int B_TILE = BN * BK * 2;   // bytes (32 KB)
@@ -136,7 +137,17 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_bf16x3_kernel(const __grid_co
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh, issued_sh, consumed_sh;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tile_m = blockIdx.y, tile_n = blockIdx.x;
+  // Grouped tile order: consecutive CTAs sweep a band of kGroupM tile rows, so
+  // the CTAs resident at one time share fewer A and B panels in L2 (bijective:
+  // the last band has min(kGroupM, rows left) rows).
+  const int nN = gridDim.x, nM = gridDim.y;
+  const int lin = blockIdx.y * nN + blockIdx.x;
+  const int per_group = kGroupM * nN;
+  const int grp = lin / per_group;
+  const int first_m = grp * kGroupM;
+  const int rows = min(kGroupM, nM - first_m);
+  const int local = lin - grp * per_group;
+  const int tile_m = first_m + local % rows, tile_n = local / rows;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
