@@ -317,7 +317,7 @@ def roofline_gemm(dev):
     torch.cuda.synchronize()
     t = e0.elapsed_time(e1) / 1e3 / reps
     achieved = 8.0 * m * n * k / t / 1e12
-    peak, src = 1613.4, "fallback"
+    peak, src = 1590.0, "fallback (no MEASURED_PEAKS.json): earlier burst measurement on this pool"
     try:
         mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak, src = float(mp["bf16_tflops"]), "measured bf16 burst"

@@ -293,6 +293,18 @@ int bem200_hmat_matvec(int n, int w, const void* x, int nl, const int32_t* lblk,
                        const void* U, const void* V, void* T, int nd, const int32_t* dblk, const int64_t* doff,
                        const void* D, void* y, void* stream);
 
+/* bem200_hmat_matvec_items: y = H x like bem200_hmat_matvec, with large blocks
+ * split over several CTAs by host-built work items: vitems (l, j0) pairs
+ * cover rows [j0, j0 + 128) of V_l (every low-rank block, all its rows;
+ * partial V^T x added into T, which is zeroed: t_len = sum kcap x w complex),
+ * bitems (b, i0) pairs cover rows [i0, i0 + 32) of block b (b < nd: dense
+ * block b, else low-rank block b - nd; every row of every block). */
+int bem200_hmat_matvec_items(int n, int w, const void* x, int nl, const int32_t* lblk, const int64_t* voff,
+                             const int64_t* uoff, const int64_t* toff, const int32_t* kcap, const int32_t* rank,
+                             const void* U, const void* V, void* T, int64_t t_len, int nd, const int32_t* dblk,
+                             const int64_t* doff, const void* D, int nvitems, const int32_t* vitems, int nbitems,
+                             const int32_t* bitems, void* y, void* stream);
+
 /* bem200_hmat_compress_green: the dense leaves and the ACA of the low-rank
  * blocks of BEM matrix `which` (0 = G1, 1 = G2, 2 = H1, 3 = H2) with every
  * entry computed on demand from the Green function, so no n x n matrix is

@@ -81,6 +81,9 @@ _SIGS = {
                                        ctypes.c_int, ctypes.c_int, _vp]),
     "bem200_hmat_matvec": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
                                           _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "bem200_hmat_matvec_items": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                                _vp, _vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, _vp, _vp,
+                                                ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp]),
     "bem200_hmat_compress_green": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int,
                                                   _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp,
                                                   ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp,

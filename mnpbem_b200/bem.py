@@ -7,7 +7,7 @@ Everything per wavelength runs in libbem200 on the GPU:
 * ``precision='fp64'`` (default): complex128 assembly, LU factors, Sigma /
   Delta build and the Eq. (19, 20) solve -- the drop-in path;
 * ``precision='mixed'``: complex64 factors built with tcgen05 tensor-core
-  GEMMs (``engine='bf16x3'`` or ``'tf32'``; ``'simt'`` uses CUDA cores),
+  GEMMs (``engine='bf16x3'``; ``'simt'`` uses CUDA cores),
   then iterative refinement against the complex128 BEM operator until the
   max-norm residual drops below ``ir_tol`` times the right-hand side.
 
@@ -21,7 +21,7 @@ from . import _native as nat
 from .greenfun import CompGreenRet
 from .planewave import CompStruct
 
-_ENGINES = {"simt": 0, "bf16x3": 1, "tf32": 2}
+_ENGINES = {"simt": 0, "bf16x3": 1}
 
 
 def _torch():

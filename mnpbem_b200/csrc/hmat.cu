@@ -327,6 +327,137 @@ __global__ void __launch_bounds__(kHThreads) hmat_block_kernel(
   }
 }
 
+// ------------------------------------------------------- work-item product
+// The per-block kernels above give each block one CTA, so the few largest
+// admissible blocks (thousands of rows) set the kernel time.  Here large
+// blocks are split over several CTAs by host-built work items:
+//   phase A item (l, j0): rows [j0, j0 + kVtRows) of V_l; the partial
+//     V_l^T x over those rows is added into T_l with FP64 atomics (T zeroed).
+//     x rows are staged in shared memory; lanes own 32 outputs (l, q) of T_l,
+//     warps split the rows, and the 8 warp partials are summed in shared memory.
+//   phase B item (b, i0): rows [i0, i0 + 32) of block b (b < nd dense, else
+//     low-rank b - nd), with the row kernel of hmat_block_kernel.
+constexpr int kVtRows = 128;
+constexpr int kItemRows = 4 * (kHThreads / 32);  // 32 rows: one pass of 8 warps x 4 rows
+
+template <int W>
+__global__ void __launch_bounds__(kHThreads) hmat_vt_items_kernel(
+    const int32_t* __restrict__ items, int w, const int32_t* __restrict__ blk, const int64_t* __restrict__ voff,
+    const int64_t* __restrict__ toff, const int32_t* __restrict__ kcap_arr, const int32_t* __restrict__ rank_arr,
+    const double2* __restrict__ x, const double2* __restrict__ Vg, double2* __restrict__ T) {
+  __shared__ double2 xs[kVtRows][W + 1];
+  __shared__ double2 red[kHThreads / 32][32];
+  const int l = items[2 * blockIdx.x], j0 = items[2 * blockIdx.x + 1];
+  const int c0 = blk[4 * l + 2], nb = blk[4 * l + 3];
+  const int kc = kcap_arr[l], r = rank_arr[l];
+  const int jn = min(kVtRows, nb - j0);
+  const double2* V = Vg + voff[l] + (long long)j0 * kc;
+  double2* Tb = T + toff[l] * w;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int e = tid; e < jn * w; e += kHThreads) {
+    const int jj = e / w, q = e % w;
+    xs[jj][q] = x[(long long)(c0 + j0 + jj) * w + q];
+  }
+  __syncthreads();
+  const int rw = r * w;
+  for (int ot = 0; ot < rw; ot += 32) {
+    const int o = ot + lane;
+    const bool ok = o < rw;
+    const int lo = ok ? o / w : 0, q = ok ? o % w : 0;
+    double2 acc = make_double2(0, 0);
+    if (ok) {
+#pragma unroll 4
+      for (int jj = wid; jj < jn; jj += kHThreads / 32) acc = cadd(acc, cmul(V[(long long)jj * kc + lo], xs[jj][q]));
+    }
+    red[wid][lane] = acc;
+    __syncthreads();
+    if (wid == 0 && ok) {
+      double2 sum = red[0][lane];
+#pragma unroll
+      for (int k = 1; k < kHThreads / 32; ++k) sum = cadd(sum, red[k][lane]);
+      double* out = reinterpret_cast<double*>(Tb + o);
+      atomicAdd(out, sum.x);
+      atomicAdd(out + 1, sum.y);
+    }
+    __syncthreads();
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(kHThreads) hmat_block_items_kernel(
+    const int32_t* __restrict__ items, int nd, int w, const double2* __restrict__ x,
+    const int32_t* __restrict__ lblk, const int64_t* __restrict__ uoff, const int64_t* __restrict__ toff,
+    const int32_t* __restrict__ kcap_arr, const int32_t* __restrict__ rank_arr, const double2* __restrict__ Ug,
+    const double2* __restrict__ T, const int32_t* __restrict__ dblk, const int64_t* __restrict__ doff,
+    const double2* __restrict__ D, double2* __restrict__ y) {
+  __shared__ double2 Ss[kSChunk][W + 1];
+  const int b = items[2 * blockIdx.x], i0 = items[2 * blockIdx.x + 1];
+  int r0, m, K, ldm;
+  const double2* M;
+  const double2* S;
+  if (b < nd) {
+    r0 = dblk[4 * b];
+    m = dblk[4 * b + 1];
+    K = dblk[4 * b + 3];
+    ldm = K;
+    M = D + doff[b];
+    S = x + (long long)dblk[4 * b + 2] * w;
+  } else {
+    const int l = b - nd;
+    r0 = lblk[4 * l];
+    m = lblk[4 * l + 1];
+    K = rank_arr[l];
+    ldm = kcap_arr[l];
+    M = Ug + uoff[l];
+    S = T + toff[l] * w;
+  }
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int js = lane & 7, rs = lane >> 3;  // 8 lanes per row, 4 rows per warp
+  const int rl = i0 + 4 * wid + rs;
+  const bool rok = rl < m;
+  double2 acc[W];
+#pragma unroll
+  for (int q = 0; q < W; ++q) acc[q] = make_double2(0, 0);
+  for (int k0 = 0; k0 < K; k0 += kSChunk) {
+    const int kn = min(kSChunk, K - k0);
+    __syncthreads();
+    for (int e = tid; e < kn * w; e += kHThreads) {
+      const int j = e / w, q = e % w;
+      Ss[j][q] = S[(long long)(k0 + j) * w + q];
+    }
+    __syncthreads();
+    if (rok) {
+      const double2* mrow = M + (long long)rl * ldm + k0;
+#pragma unroll 4
+      for (int j = js; j < kn; j += 8) {
+        const double2 a = mrow[j];
+#pragma unroll
+        for (int q = 0; q < W; ++q)
+          if (q < w) acc[q] = cadd(acc[q], cmul(a, Ss[j][q]));
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < W; ++q) {
+    double2 v = acc[q];
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+      v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    acc[q] = v;
+  }
+  if (rok) {
+#pragma unroll
+    for (int q = 0; q < W; ++q)
+      if (q < w && q % 8 == js) {
+        double* out = reinterpret_cast<double*>(y + (long long)(r0 + rl) * w + q);
+        atomicAdd(out, acc[q].x);
+        atomicAdd(out + 1, acc[q].y);
+      }
+  }
+}
+
 }  // namespace bem200
 
 using namespace bem200;
@@ -450,6 +581,41 @@ int bem200_hmat_matvec(int n, int w, const void* x, int nl, const int32_t* lblk,
     hmat_block_kernel<16><<<nd + nl, kHThreads, 0, s>>>(nd, w, (const double2*)x, lblk, uoff, toff, kcap, rank,
                                                         (const double2*)U, (const double2*)T, dblk, doff,
                                                         (const double2*)D, (double2*)y);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+int bem200_hmat_matvec_items(int n, int w, const void* x, int nl, const int32_t* lblk, const int64_t* voff,
+                             const int64_t* uoff, const int64_t* toff, const int32_t* kcap, const int32_t* rank,
+                             const void* U, const void* V, void* T, int64_t t_len, int nd, const int32_t* dblk,
+                             const int64_t* doff, const void* D, int nvitems, const int32_t* vitems, int nbitems,
+                             const int32_t* bitems, void* y, void* stream) {
+  BEM_REQUIRE(n > 0 && w > 0 && w <= 16 && x && y && nl >= 0 && nd >= 0 && nvitems >= 0 && nbitems >= 0 &&
+                  t_len >= 0,
+              BEM200_ERR_ARG, "hmat_matvec_items: bad arguments (w <= 16 columns)");
+  BEM_REQUIRE((nvitems == 0 || (vitems && T && V && lblk)) && (nbitems == 0 || bitems), BEM200_ERR_ARG,
+              "hmat_matvec_items: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  BEM_CUDA_CHECK(cudaMemsetAsync(y, 0, sizeof(double2) * (size_t)n * w, s));
+  if (nvitems > 0) {
+    BEM_CUDA_CHECK(cudaMemsetAsync(T, 0, sizeof(double2) * (size_t)t_len, s));
+    if (w <= 8)
+      hmat_vt_items_kernel<8><<<nvitems, kHThreads, 0, s>>>(vitems, w, lblk, voff, toff, kcap, rank,
+                                                            (const double2*)x, (const double2*)V, (double2*)T);
+    else
+      hmat_vt_items_kernel<16><<<nvitems, kHThreads, 0, s>>>(vitems, w, lblk, voff, toff, kcap, rank,
+                                                             (const double2*)x, (const double2*)V, (double2*)T);
+    BEM_LAUNCH_CHECK();
+  }
+  if (nbitems == 0) return BEM200_OK;
+  if (w <= 8)
+    hmat_block_items_kernel<8><<<nbitems, kHThreads, 0, s>>>(bitems, nd, w, (const double2*)x, lblk, uoff, toff,
+                                                             kcap, rank, (const double2*)U, (const double2*)T, dblk,
+                                                             doff, (const double2*)D, (double2*)y);
+  else
+    hmat_block_items_kernel<16><<<nbitems, kHThreads, 0, s>>>(bitems, nd, w, (const double2*)x, lblk, uoff, toff,
+                                                              kcap, rank, (const double2*)U, (const double2*)T, dblk,
+                                                              doff, (const double2*)D, (double2*)y);
   BEM_LAUNCH_CHECK();
   return BEM200_OK;
 }

@@ -223,6 +223,14 @@ class HMatrixGPU:
         self.c2p = t(tree.ind[:, 0].astype(np.int32))
         self.p2c = t(tree.ind[:, 1].astype(np.int32))
         self.ranks = None
+        # work items of the product: (low-rank block, first V row) per 128 rows
+        # of V, and (block, first row) per 32 rows of every block (dense first)
+        vit = [(l, j0) for l in range(len(lb)) for j0 in range(0, int(lb[l, 3]), 128)]
+        bit = [(b, i0) for b in range(len(db)) for i0 in range(0, int(db[b, 1]), 32)]
+        bit += [(len(db) + l, i0) for l in range(len(lb)) for i0 in range(0, int(lb[l, 1]), 32)]
+        self.nvitems, self.nbitems = len(vit), len(bit)
+        self.vitems = t(np.array(vit, dtype=np.int32).reshape(-1))
+        self.bitems = t(np.array(bit, dtype=np.int32).reshape(-1))
 
     def compress(self, M, scratch=None):
         """Compress the dense n x n complex128 device matrix M (particle order)."""
@@ -272,7 +280,21 @@ class HMatrixGPU:
         return ne / float(self.n * self.n)
 
     def matvec(self, x, y, w):
-        """y = H x, x and y n x w row-major complex128 in cluster order."""
+        """y = H x, x and y n x w row-major complex128 in cluster order, with
+        large blocks split over several CTAs (bem200_hmat_matvec_items)."""
+        torch = _torch()
+        tbuf = getattr(self, "_tbuf", None)
+        need = max(int(np.sum(self._kcap)) * w, 1)
+        if tbuf is None or tbuf.numel() < need:
+            self._tbuf = tbuf = torch.empty(need, dtype=torch.complex128, device=self.dev)
+        nat.call("bem200_hmat_matvec_items", self.n, w, nat.ptr(x), self.nlow, nat.ptr(self.lblk),
+                 nat.ptr(self.voff), nat.ptr(self.uoff), nat.ptr(self.toff), nat.ptr(self.kcap), nat.ptr(self.rank),
+                 nat.ptr(self.U), nat.ptr(self.V), nat.ptr(tbuf), int(np.sum(self._kcap)) * w, self.ndense,
+                 nat.ptr(self.dblk), nat.ptr(self.doff), nat.ptr(self.D), self.nvitems, nat.ptr(self.vitems),
+                 self.nbitems, nat.ptr(self.bitems), nat.ptr(y), nat.stream_ptr())
+
+    def matvec_per_block(self, x, y, w):
+        """y = H x with one CTA per block (bem200_hmat_matvec)."""
         torch = _torch()
         tbuf = getattr(self, "_tbuf", None)
         need = max(int(np.sum(self._kcap)) * w, 1)

@@ -377,7 +377,7 @@ def main(argv=None):
     if not torch.cuda.is_available():
         raise RuntimeError("microbench needs a CUDA device")
     if a.case == "step":
-        a.engine = {0: "simt", 1: "bf16x3", 2: "tf32"}[a.engine]
+        a.engine = {0: "simt", 1: "bf16x3"}[a.engine]
     out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf, "hmat": case_hmat,
            "iter": case_iter, "large": case_large, "sweep": case_sweep,
            "shape": case_shape}[a.case](a)

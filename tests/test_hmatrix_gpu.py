@@ -81,6 +81,10 @@ def test_gpu_hmatrix_matvec(cuda, tag, w):
     y[c2p] = yc.cpu().numpy()
     assert rel(y, full @ x) < 1e-13
     assert rel(y, G1 @ x) < 1e-5
+    # the one-CTA-per-block product agrees (FP64 atomics: summation order differs)
+    yb = torch.empty_like(xc)
+    h.matvec_per_block(xc, yb, w)
+    assert rel(yb.cpu().numpy(), yc.cpu().numpy()) < 1e-13
 
 
 @pytest.mark.parametrize("mk", ["sphere", "dimer"])
