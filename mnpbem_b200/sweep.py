@@ -20,7 +20,7 @@ fill 148 SMs alone, run beside it.  Two schedules:
 Every per-wavelength step stays on the GPU (right-hand side, factors, solve
 with FP64 refinement, far fields); only the (npol,) cross sections return.
 
-``uneven_meshes(seed)`` builds the survey's uneven batch with the reference's
+``uneven_meshes(seed)`` builds a seeded batch of uneven meshes with the reference's
 generators: spheres (trisphere, curved), ellipsoids (triellipsoid, flat) and
 capped rods (trirod, curved) with face counts 284 ... 5768, seeded sizes and
 gold or silver Drude metals.
