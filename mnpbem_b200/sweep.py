@@ -93,52 +93,96 @@ def lpt(costs, workers):
     return parts
 
 
-def sweep_plan(sizes, nlambda, workers, schedule="interleave"):
-    """Per worker, the list of (mesh index, wavelength indices) it solves."""
+def sweep_plan(sizes, nlambda, workers, schedule="interleave", units=None):
+    """Per worker, the list of (mesh index, wavelength indices) it solves.
+    ``units`` (mesh -> wavelength indices) restricts the plan to a share of
+    the (mesh, wavelength) work; by default every mesh at every wavelength."""
     nm = len(sizes)
+    if units is None:
+        units = {m: np.arange(nlambda) for m in range(nm)}
+    meshes = [m for m in range(nm) if len(units.get(m, ())) > 0]
     if schedule == "mesh":
-        parts = lpt([float(n) ** 3 for n in sizes], workers)
-        return [[(m, np.arange(nlambda)) for m in parts[w]] for w in range(workers)]
+        parts = lpt([float(sizes[m]) ** 3 for m in meshes], workers)
+        return [[(meshes[i], np.asarray(units[meshes[i]])) for i in parts[w]] for w in range(workers)]
     if schedule != "interleave":
         raise ValueError("sweep_plan: schedule must be 'interleave' or 'mesh'")
-    order = sorted(range(nm), key=lambda m: -sizes[m])
+    order = sorted(meshes, key=lambda m: -sizes[m])
     plan = []
     for w in range(workers):
-        r = (w * nm) // workers
-        plan.append([(m, np.arange(w, nlambda, workers)) for m in order[r:] + order[:r]])
+        r = (w * len(order)) // workers
+        items = [(m, np.asarray(units[m])[w::workers]) for m in order[r:] + order[:r]]
+        plan.append([(m, lam) for m, lam in items if len(lam)])
     return plan
 
 
-def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=4, engine="bf16x3", schedule="interleave",
-                **bem_kwargs):
-    """Extinction and scattering of every particle at every wavelength.
+def partition_units(sizes, nlambda, world):
+    """Longest processing time first over the (mesh, wavelength) units with
+    cost n^3: for each rank, a dict mesh -> sorted wavelength indices."""
+    units = [(m, i) for m in range(len(sizes)) for i in range(nlambda)]
+    parts = lpt([float(sizes[m]) ** 3 for m, _ in units], world)
+    out = []
+    for p in parts:
+        d = {}
+        for u in p:
+            m, i = units[u]
+            d.setdefault(m, []).append(i)
+        out.append({m: np.array(sorted(v)) for m, v in d.items()})
+    return out
 
-    Returns a dict: ext, sca ((nmesh, nlambda, npol) arrays), setup_s (BEMRet
+
+class _BEMSolver:
+    """(mesh, wavelength) -> (ext, sca) with one resident BEMRet per mesh."""
+
+    def __init__(self, particle, pol, dirs, precision, engine, **bem_kwargs):
+        from .bem import BEMRet
+        from .planewave import PlaneWaveRet
+        self.bem = BEMRet(particle, precision=precision, engine=engine, **bem_kwargs)
+        self.exc = PlaneWaveRet(pol, dirs)
+
+    def prepare(self):
+        self.bem._alloc()    # workspaces now, not inside the timed loops
+
+    def __call__(self, enei):
+        r = self.bem.cross_sections(self.exc, float(enei))
+        return r["ext"], r["sca"]
+
+
+def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=4, engine="bf16x3", schedule="interleave",
+                units=None, solver_factory=None, **bem_kwargs):
+    """Extinction and scattering of every particle at every wavelength (or of
+    the (mesh, wavelength) ``units`` given, mesh -> wavelength indices; the
+    others stay 0).
+
+    Returns a dict: ext, sca ((nmesh, nlambda, npol) arrays), setup_s (solver
     construction for every (worker, mesh) pair: refinement tables,
-    workspaces), sweep_s (the wavelength loops, all workers), solves
-    (nmesh * nlambda * npol), solves_per_s (solves / sweep_s), per_worker
-    seconds and the plan."""
+    workspaces), sweep_s (the wavelength loops, all workers), solves (units x
+    npol), solves_per_s (solves / sweep_s), per_worker seconds and the plan.
+    ``solver_factory(particle, pol, dirs)`` may replace the GPU solver (an
+    object called with a wavelength, returning (ext, sca))."""
     import torch
-    from .bem import BEMRet
-    from .planewave import PlaneWaveRet
     enei = np.asarray(enei, dtype=float).ravel()
     pol = np.atleast_2d(np.asarray(pol, dtype=float))
     dirs = np.atleast_2d(np.asarray(dirs, dtype=float))
     npol = pol.shape[0]
     nm = len(particles)
+    cuda = solver_factory is None
+    if cuda:
+        def solver_factory(p, pol_, dirs_):
+            return _BEMSolver(p, pol_, dirs_, precision, engine, **bem_kwargs)
     workers = max(1, int(workers))
     if schedule == "mesh":
         workers = min(workers, nm)
     else:
         workers = min(workers, len(enei))
-    plan = sweep_plan([p.n for p in particles], len(enei), workers, schedule)
+    plan = sweep_plan([p.n for p in particles], len(enei), workers, schedule, units)
     t0 = time.perf_counter()
-    bems = [{m: BEMRet(particles[m], precision=precision, engine=engine, **bem_kwargs) for m, _ in plan[w]}
-            for w in range(workers)]
-    for per in bems:
-        for b in per.values():
-            b._alloc()    # workspaces now, not inside the timed loops
-    torch.cuda.synchronize()
+    solvers = [{m: solver_factory(particles[m], pol, dirs) for m, _ in plan[w]} for w in range(workers)]
+    for per in solvers:
+        for s_ in per.values():
+            if hasattr(s_, "prepare"):
+                s_.prepare()
+    if cuda:
+        torch.cuda.synchronize()
     setup = time.perf_counter() - t0
     ext = np.zeros((nm, len(enei), npol))
     sca = np.zeros_like(ext)
@@ -148,16 +192,16 @@ def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=4, engine
 
     def run(w):
         try:
-            stream = torch.cuda.Stream()
-            exc = PlaneWaveRet(pol, dirs)
+            stream = torch.cuda.Stream() if cuda else None
             start.wait()
             tw = time.perf_counter()
-            with torch.cuda.stream(stream):
+            ctx = torch.cuda.stream(stream) if cuda else _nullcontext()
+            with ctx:
                 for m, lam in plan[w]:
                     for i in lam:
-                        r = bems[w][m].cross_sections(exc, float(enei[i]))
-                        ext[m, i], sca[m, i] = r["ext"], r["sca"]
-                stream.synchronize()
+                        ext[m, i], sca[m, i] = solvers[w][m](enei[i])
+                if cuda:
+                    stream.synchronize()
             per_worker[w] = time.perf_counter() - tw
         except BaseException as exc_:  # reported on the calling thread
             errors.append(exc_)
@@ -174,11 +218,48 @@ def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=4, engine
     t1 = time.perf_counter()
     for t in threads:
         t.join()
-    torch.cuda.synchronize()
+    if cuda:
+        torch.cuda.synchronize()
     sweep = time.perf_counter() - t1
     if errors:
         raise errors[0]
-    solves = nm * len(enei) * npol
+    solves = sum(len(lam) for p in plan for _, lam in p) * npol
     return {"ext": ext, "sca": sca, "setup_s": setup, "sweep_s": sweep, "solves": solves,
-            "solves_per_s": solves / sweep, "per_worker_s": per_worker,
+            "solves_per_s": solves / sweep if sweep > 0 else float("inf"), "per_worker_s": per_worker,
             "plan": [[(int(m), len(lam)) for m, lam in p] for p in plan]}
+
+
+class _nullcontext:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def solve_sweep_dist(particles, enei, pol, dirs, device=None, **kw):
+    """The uneven sweep inside an initialised process group, one rank per GPU:
+    the (mesh, wavelength) units are split over the ranks by longest
+    processing time first (cost n^3, ``partition_units``), every rank runs
+    ``solve_sweep`` on its share, and two all-reduces (SUM of the zero-padded
+    cross sections, MAX of the sweep time) give every rank the whole result.
+    No other exchange: the units are independent."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size() if dist.is_initialized() else 1
+    rank = dist.get_rank() if dist.is_initialized() else 0
+    enei = np.asarray(enei, dtype=float).ravel()
+    share = partition_units([p.n for p in particles], len(enei), world)[rank]
+    r = solve_sweep(particles, enei, pol, dirs, units=share, **kw)
+    buf = torch.as_tensor(np.stack([r["ext"], r["sca"]]), device=device)
+    wall = torch.tensor([r["sweep_s"]], dtype=torch.float64, device=device)
+    solves = torch.tensor([float(r["solves"])], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(buf, op=dist.ReduceOp.SUM)
+        dist.all_reduce(wall, op=dist.ReduceOp.MAX)
+        dist.all_reduce(solves, op=dist.ReduceOp.SUM)
+    out = buf.cpu().numpy()
+    w = float(wall.item())
+    n = int(solves.item())
+    return {"ext": out[0], "sca": out[1], "sweep_s": w, "solves": n, "solves_per_s": n / w if w > 0 else float("inf"),
+            "share": {int(m): v.tolist() for m, v in share.items()}}
