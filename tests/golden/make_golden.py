@@ -25,6 +25,9 @@ input/output vectors that pin the oracle and the geometry module:
                           ACA ranks / errors for the sphere and the small dimer.
 * ``meshes.npz``        : face arrays of the reference mesh generators; ext / sca of a
                           small curved rod, rounded cube and flat ellipsoid.
+* ``matlab_rod.npz``    : MNPBEM17 MATLAB and reference-Python ext / sca of the gold rod
+                          trirod(10, 40, [15, 15, 15]) (validation/03_bemret/rod) and the
+                          tabulated-gold eps at those wavelengths.
 
 Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only] [--meshes-only]
 """
@@ -146,6 +149,21 @@ def matlab_cfg0():
     save("matlab_cfg0.npz", enei=data[:, 0], ext=data[:, 1], sca=data[:, 2], absorption=data[:, 3], eps_gold=eps)
 
 
+def matlab_rod():
+    """MNPBEM17 (MATLAB) and reference-Python ext / sca of the curved gold rod
+    trirod(10, 40, [15, 15, 15]) in vacuum, tabulated gold, x-pol along +z and
+    z-pol along +x, 41 wavelengths 400-800 nm
+    (validation/03_bemret/rod/data/bemret_{matlab,python}.csv), with the
+    reference EpsTable('gold.dat') eps at those wavelengths."""
+    d = os.path.join(_refenv.REFERENCE_ROOT, "validation", "03_bemret", "rod", "data")
+    m = np.loadtxt(os.path.join(d, "bemret_matlab.csv"), delimiter=",", skiprows=1)
+    p = np.loadtxt(os.path.join(d, "bemret_python.csv"), delimiter=",", skiprows=1)
+    gold = EpsTable("gold.dat")
+    eps = np.array([complex(np.asarray(gold(e)[0]).ravel()[0]) for e in m[:, 0]])
+    save("matlab_rod.npz", enei=m[:, 0], matlab=m[:, 1:], python=p[:, 1:], eps_gold=eps,
+         columns=np.array(["ext_x", "sca_x", "ext_z", "sca_z"]))
+
+
 def dimer_cfg1():
     p = _dimer(1444, 40.0, 1.0)
     t0 = time.time()
@@ -265,11 +283,13 @@ def meshes():
 if __name__ == "__main__":
     if "--meshes-only" in sys.argv:
         meshes()
+        matlab_rod()
         sys.exit(0)
     hmat_trees()
     if "--hmat-only" in sys.argv:
         sys.exit(0)
     meshes()
+    matlab_rod()
     geom()
     refined_cfg0()
     matrices_s60()

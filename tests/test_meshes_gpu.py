@@ -90,3 +90,23 @@ def test_uneven_sweep_two_workers(cuda):
             sig, _ = ref.solve(exc.potential(cp, float(e)))
             assert rel(r2["ext"][m, i], exc.extinction(sig)) < 1e-8
             assert rel(r2["sca"][m, i], exc.scattering(sig)[0]) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_rod_matches_mnpbem17(cuda, precision):
+    """The gold rod trirod(10, 40, [15, 15, 15]) (588 curved faces, vacuum,
+    tabulated gold, x-pol along +z and z-pol along +x) against MNPBEM17
+    (MATLAB) at 5 of the 41 wavelengths of the reference's validation CSV."""
+    from mnpbem_b200 import BEMRet, PlaneWaveRet
+    from mnpbem_b200.geometry import ComParticle, trirod
+    from mnpbem_b200.materials import EpsConst, EpsValues
+    g = golden("matlab_rod.npz")
+    cp = ComParticle([EpsConst(1.0), EpsValues(dict(zip(g["enei"], g["eps_gold"])))],
+                     [trirod(10.0, 40.0, [15, 15, 15])], [[2, 1]], 1, interp="curv")
+    bem = BEMRet(cp, precision=precision)
+    exc = PlaneWaveRet(POL, DIR)
+    for i in (0, 10, 20, 30, 40):
+        sig, bem = bem.solve(exc.potential(cp, float(g["enei"][i])))
+        ext, sca = exc.extinction(sig), exc.scattering(sig)[0]
+        got = np.array([ext[0], sca[0], ext[1], sca[1]])
+        assert np.max(np.abs(got - g["matlab"][i]) / np.abs(g["matlab"][i])) < 1e-9, (i, got, g["matlab"][i])
