@@ -28,6 +28,8 @@ input/output vectors that pin the oracle and the geometry module:
 * ``matlab_rod.npz``    : MNPBEM17 MATLAB and reference-Python ext / sca of the gold rod
                           trirod(10, 40, [15, 15, 15]) (validation/03_bemret/rod) and the
                           tabulated-gold eps at those wavelengths.
+* ``matlab_iter.npz``   : MNPBEM17 MATLAB direct and iterative (bemiter) ext of
+                          trisphere(144, 20) with tabulated gold (validation/08_iterative).
 
 Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only] [--meshes-only]
 """
@@ -164,6 +166,17 @@ def matlab_rod():
          columns=np.array(["ext_x", "sca_x", "ext_z", "sca_z"]))
 
 
+def matlab_iter():
+    """MNPBEM17 (MATLAB) direct and iterative (bemiter) retarded extinction of
+    trisphere(144, 20) in vacuum with tabulated gold, x-pol along +z, 41
+    wavelengths 400-800 nm (validation/08_iterative/sphere/data/ret_matlab.csv)."""
+    csv = os.path.join(_refenv.REFERENCE_ROOT, "validation", "08_iterative", "sphere", "data", "ret_matlab.csv")
+    m = np.loadtxt(csv, delimiter=",", skiprows=1)
+    gold = EpsTable("gold.dat")
+    eps = np.array([complex(np.asarray(gold(e)[0]).ravel()[0]) for e in m[:, 0]])
+    save("matlab_iter.npz", enei=m[:, 0], ext_direct=m[:, 1], ext_iter=m[:, 2], eps_gold=eps)
+
+
 def dimer_cfg1():
     p = _dimer(1444, 40.0, 1.0)
     t0 = time.time()
@@ -284,12 +297,14 @@ if __name__ == "__main__":
     if "--meshes-only" in sys.argv:
         meshes()
         matlab_rod()
+        matlab_iter()
         sys.exit(0)
     hmat_trees()
     if "--hmat-only" in sys.argv:
         sys.exit(0)
     meshes()
     matlab_rod()
+    matlab_iter()
     geom()
     refined_cfg0()
     matrices_s60()
