@@ -229,6 +229,24 @@ def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=4, engine
             "plan": [[(int(m), len(lam)) for m, lam in p] for p in plan]}
 
 
+def autotune_sweep(particles, enei, pol, dirs, candidates=((2, "interleave"), (4, "interleave"), (8, "interleave"),
+                                                          (2, "mesh")), probe=4, **kw):
+    """Pick the (workers, schedule) of ``solve_sweep`` for this batch by timing
+    each candidate on ``probe`` wavelengths spread over the sweep (every mesh
+    at each of them).  Returns (best candidate, {candidate: solves/s}).  The
+    probe solves are real solves; their cost is a few wavelengths per
+    candidate, against the whole sweep."""
+    enei = np.asarray(enei, dtype=float).ravel()
+    pick = np.unique(np.linspace(0, len(enei) - 1, max(1, min(probe, len(enei)))).round().astype(int))
+    units = {m: pick for m in range(len(particles))}
+    rates = {}
+    for workers, schedule in candidates:
+        r = solve_sweep(particles, enei, pol, dirs, workers=workers, schedule=schedule, units=units, **kw)
+        rates[(workers, schedule)] = r["solves_per_s"]
+    best = max(rates, key=rates.get)
+    return best, rates
+
+
 class _nullcontext:
     def __enter__(self):
         return self

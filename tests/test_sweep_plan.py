@@ -117,3 +117,31 @@ def test_uneven_sweep_two_gloo_ranks(tmp_path):
         for mi, n in enumerate(sizes):
             np.testing.assert_array_equal(d["ext"][mi, :, 0], n + enei)
         assert int(d["solves"]) == len(sizes) * len(enei)
+
+
+def test_autotune_picks_the_fastest_schedule():
+    """autotune_sweep with a stand-in solver whose time per call grows with
+    the number of concurrent workers beyond 4: the 4-worker interleave wins."""
+    import threading
+    import time as _time
+    from mnpbem_b200.sweep import autotune_sweep
+    active = [0]
+    lock = threading.Lock()
+
+    def factory(p, pol, dirs):
+        def solve(enei):
+            with lock:
+                active[0] += 1
+                k = active[0]
+            _time.sleep(0.004 * max(1, k - 3))      # contention above 4 concurrent solves
+            with lock:
+                active[0] -= 1
+            return np.zeros(len(pol)), np.zeros(len(pol))
+        return solve
+
+    meshes = [_Mesh(n) for n in (284, 760, 1296, 2000, 2884, 3600, 4800, 5768)]
+    best, rates = autotune_sweep(meshes, np.linspace(450, 900, 128), [[1, 0, 0]], [[0, 0, 1]], probe=16,
+                                 candidates=((1, "interleave"), (4, "interleave"), (16, "interleave")),
+                                 solver_factory=factory)
+    assert set(rates) == {(1, "interleave"), (4, "interleave"), (16, "interleave")}
+    assert best == (4, "interleave"), rates
