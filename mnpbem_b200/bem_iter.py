@@ -26,7 +26,7 @@ import ctypes
 import numpy as np
 
 from . import _native as nat
-from .bem import BEMRet, _ENGINES, _excitation_rhs
+from .bem import BEMRet, _ENGINES
 from .planewave import CompStruct
 
 
