@@ -8,6 +8,8 @@ the path that ``mnpbem_b200`` runs on the GPU (MNPBEM, Python port v1.6.2):
 * Green matrices G1, G2, H1, H2  -> ``oracle.green``  (a6)
 * BEMRet init / excitation / solve, full 8N operator -> ``oracle.bem`` (a7-a10)
 * plane-wave potentials, far field, extinction, scattering -> ``oracle.farfield``
+* transposed solve and reverse-mode geometry derivatives (no reference
+  counterpart; checked by adjoint identities)        -> ``oracle.adjoint``
 
 Every function cites the reference file:line it follows.  The oracle is
 pinned against golden vectors produced by the reference itself
