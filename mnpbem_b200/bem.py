@@ -277,3 +277,13 @@ class BEMRet:
     def clear(self):
         self.enei = None
         return self
+
+    def potential(self, sig, inout=2):
+        """Potentials of a solution at the faces (reference bem_ret.py:1833,
+        via CompGreenRet.potential): not provided by this library."""
+        raise NotImplementedError("BEMRet.potential: surface potentials of a solution are not implemented on the GPU")
+
+    def field(self, sig, inout=2):
+        """Fields of a solution (reference bem_ret.py:1861, via CompGreenRet.field
+        and the Cartesian-derivative Green functions): not provided."""
+        raise NotImplementedError("BEMRet.field: fields of a solution are not implemented on the GPU")
