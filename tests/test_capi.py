@@ -31,3 +31,11 @@ def test_version_and_error_string():
     st = _native.lib().bem200_refine_count(0, None, None, 0.0, 3.0, None, None)
     assert st == 1
     assert "refine_count" in _native.last_error()
+
+
+def test_every_declared_symbol_has_a_ctypes_signature():
+    """Calls through mnpbem_b200._native use explicit argument types (doubles
+    and 64-bit sizes would be mangled by ctypes' defaults)."""
+    from mnpbem_b200 import _native
+    missing = [s for s in declared_symbols() if s not in _native._SIGS]
+    assert not missing, missing
