@@ -9,6 +9,10 @@
 ``pinfty256.npz`` : the 256-direction unit sphere used for far-field
                     integration (directions, solid-angle weights, centroids),
                     shipped by MNPBEM as ``mnpbem/data/pinfty256.bin``.
+``eps_tables.npz``: the tabulated optical constants (photon energy in eV, n, k)
+                    that MNPBEM ships as ``mnpbem/materials/data/*.dat``: gold
+                    and silver of Johnson & Christy, gold, silver and copper of
+                    Palik.  ``EpsTable('gold.dat')`` reads them by name.
 
 Run once in a checkout that has the MNPBEM sources next to it:
     python mnpbem_b200/data/make_data.py /path/to/MNPBEM
@@ -46,6 +50,25 @@ def main(root):
         pos = nvec.copy()
         area = tail[:n]
     np.savez_compressed(os.path.join(here, "pinfty256.npz"), nvec=nvec, area=area, pos=pos)
+    tables = {}
+    mdir = os.path.join(root, "mnpbem", "materials", "data")
+    for name in sorted(os.listdir(mdir)):
+        if not name.endswith(".dat"):
+            continue
+        rows = []
+        with open(os.path.join(mdir, name)) as f:
+            for line in f:
+                line = line.strip()
+                if not line or line[0] in "%#":
+                    continue
+                try:
+                    vals = [float(x) for x in line.split()]
+                except ValueError:
+                    continue
+                if len(vals) >= 3:
+                    rows.append(vals[:3])
+        tables[name] = np.array(rows)
+    np.savez_compressed(os.path.join(here, "eps_tables.npz"), **tables)
 
 
 if __name__ == "__main__":

@@ -45,28 +45,45 @@ class EpsDrude:
         return "EpsDrude({}, {}, {})".format(self.eps0, self.wp, self.gammad)
 
 
+def _bundled_tables():
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "eps_tables.npz")
+    return np.load(path) if os.path.exists(path) else {}
+
+
 class EpsTable:
     """Tabulated refractive index (columns: energy [eV], n, k), cubic-spline
     interpolated in wavelength; eps = (n + i k)^2.  Raises ValueError outside
-    the tabulated range, like the reference."""
+    the tabulated range, like the reference (mnpbem/materials/eps_table.py).
+
+    ``filename`` is a path, or the name of one of the tables the reference
+    ships: 'gold.dat', 'silver.dat' (Johnson & Christy), 'goldpalik.dat',
+    'silverpalik.dat', 'copperpalik.dat' (Palik)."""
 
     def __init__(self, filename):
         from scipy.interpolate import CubicSpline
-        if not os.path.exists(filename):
-            raise FileNotFoundError("Material data file not found: {}".format(filename))
-        rows = []
-        with open(filename) as f:
-            for line in f:
-                line = line.strip()
-                if not line or line[0] in "%#":
-                    continue
-                try:
-                    vals = [float(x) for x in line.split()]
-                except ValueError:
-                    continue
-                if len(vals) >= 3:
-                    rows.append(vals[:3])
-        data = np.array(rows)
+        if os.path.exists(filename):
+            rows = []
+            with open(filename) as f:
+                for line in f:
+                    line = line.strip()
+                    if not line or line[0] in "%#":
+                        continue
+                    try:
+                        vals = [float(x) for x in line.split()]
+                    except ValueError:
+                        continue
+                    if len(vals) >= 3:
+                        rows.append(vals[:3])
+            data = np.array(rows)
+        else:
+            tables = _bundled_tables()
+            name = os.path.basename(filename)
+            if name not in tables:
+                raise FileNotFoundError("Material data file not found: {}".format(filename))
+            data = np.asarray(tables[name])
+        if len(data) == 0:
+            raise ValueError("No valid data found in {}".format(filename))
+        self.filename = os.path.basename(filename)
         enei = EV2NM / data[:, 0]
         order = np.argsort(enei)
         self.enei = enei[order]

@@ -30,6 +30,7 @@ input/output vectors that pin the oracle and the geometry module:
                           tabulated-gold eps at those wavelengths.
 * ``matlab_iter.npz``   : MNPBEM17 MATLAB direct and iterative (bemiter) ext of
                           trisphere(144, 20) with tabulated gold (validation/08_iterative).
+* ``eps_tables.npz``    : eps and k of the reference EpsTable for each of its five tables.
 
 Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only] [--meshes-only]
 """
@@ -177,6 +178,20 @@ def matlab_iter():
     save("matlab_iter.npz", enei=m[:, 0], ext_direct=m[:, 1], ext_iter=m[:, 2], eps_gold=eps)
 
 
+def eps_tables():
+    """eps and k of the reference EpsTable for every table it ships, at 25
+    wavelengths inside each table's range."""
+    out = {}
+    for name in ("gold.dat", "silver.dat", "goldpalik.dat", "silverpalik.dat", "copperpalik.dat"):
+        t = EpsTable(name)
+        lo, hi = float(t.enei.min()), float(t.enei.max())
+        enei = np.linspace(lo + 1e-6 * (hi - lo), hi - 1e-6 * (hi - lo), 25)
+        eps, k = t(enei)
+        key = name.replace(".dat", "")
+        out[key + "_enei"], out[key + "_eps"], out[key + "_k"] = enei, np.asarray(eps), np.asarray(k)
+    save("eps_tables.npz", **out)
+
+
 def dimer_cfg1():
     p = _dimer(1444, 40.0, 1.0)
     t0 = time.time()
@@ -298,6 +313,7 @@ if __name__ == "__main__":
         meshes()
         matlab_rod()
         matlab_iter()
+        eps_tables()
         sys.exit(0)
     hmat_trees()
     if "--hmat-only" in sys.argv:
@@ -305,6 +321,7 @@ if __name__ == "__main__":
     meshes()
     matlab_rod()
     matlab_iter()
+    eps_tables()
     geom()
     refined_cfg0()
     matrices_s60()

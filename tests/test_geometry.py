@@ -66,3 +66,20 @@ def test_flat_and_quad_faces():
     np.testing.assert_allclose(np.bincount(pr, weights=pw), np.ones(6), atol=1e-12)
     c = p.curved()
     np.testing.assert_allclose(c.area, np.ones(6), atol=1e-12)
+
+
+def test_eps_tables_match_reference():
+    """EpsTable by name reads the tables the reference ships (regenerated by
+    mnpbem_b200/data/make_data.py) and interpolates them like the reference."""
+    import pytest
+    from conftest import golden
+    from mnpbem_b200.materials import EpsTable
+    g = golden("eps_tables.npz")
+    for name in ("gold", "silver", "goldpalik", "silverpalik", "copperpalik"):
+        eps, k = EpsTable(name + ".dat")(g[name + "_enei"])
+        np.testing.assert_allclose(eps, g[name + "_eps"], rtol=1e-14, atol=0)
+        np.testing.assert_allclose(k, g[name + "_k"], rtol=1e-14, atol=0)
+    with pytest.raises(ValueError):
+        EpsTable("gold.dat")(5000.0)
+    with pytest.raises(FileNotFoundError):
+        EpsTable("unobtainium.dat")
