@@ -30,10 +30,43 @@ class EpsConst:
 
 
 class EpsDrude:
-    """Drude metal eps = eps0 - wp^2 / (w (w + i gammad)), energies in eV."""
+    """Drude metal eps = eps0 - wp^2 / (w (w + i gammad)), energies in eV.
+
+    ``EpsDrude.gold()``, ``.silver()``, ``.aluminum()`` give MNPBEM's preset
+    metals: a free-electron (jellium) plasma energy from the electron-gas
+    parameter rs, wp = sqrt(4 pi n) Hartree with n = 3 / (4 pi rs^3) in atomic
+    units, and the toolbox's background eps0 and damping (reference
+    mnpbem/materials/eps_drude.py:126-217, MATLAB @epsdrude/init.m)."""
+
+    _HARTREE = 27.2116        # eV
+    _PRESETS = {              # rs, eps0, damping in Hartree
+        "gold": (3.0, 10.0, 0.66 / 27.2116 / 10), "silver": (3.0, 3.3, 0.66 / 27.2116 / 30),
+        "aluminum": (2.07, 1.0, 1.06 / 27.2116)}
+    _ALIASES = {"Au": "gold", "Ag": "silver", "Al": "aluminum"}
 
     def __init__(self, eps0, wp, gammad, name=None):
         self.eps0, self.wp, self.gammad, self.name = eps0, wp, gammad, name
+
+    @classmethod
+    def from_name(cls, name):
+        key = cls._ALIASES.get(name, name)
+        if key not in cls._PRESETS:
+            raise ValueError("Material name unknown: {}".format(name))
+        rs, eps0, gam = cls._PRESETS[key]
+        wp = np.sqrt(4 * np.pi * (3 / (4 * np.pi * rs ** 3)))
+        return cls(eps0=eps0, wp=wp * cls._HARTREE, gammad=gam * cls._HARTREE, name=name)
+
+    @classmethod
+    def gold(cls):
+        return cls.from_name("gold")
+
+    @classmethod
+    def silver(cls):
+        return cls.from_name("silver")
+
+    @classmethod
+    def aluminum(cls):
+        return cls.from_name("aluminum")
 
     def __call__(self, enei):
         enei = np.asarray(enei, dtype=float)

@@ -30,7 +30,8 @@ input/output vectors that pin the oracle and the geometry module:
                           tabulated-gold eps at those wavelengths.
 * ``matlab_iter.npz``   : MNPBEM17 MATLAB direct and iterative (bemiter) ext of
                           trisphere(144, 20) with tabulated gold (validation/08_iterative).
-* ``eps_tables.npz``    : eps and k of the reference EpsTable for each of its five tables.
+* ``eps_tables.npz``    : eps and k of the reference EpsTable for each of its five tables,
+                          and the parameters of its preset Drude metals.
 
 Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only] [--meshes-only]
 """
@@ -189,6 +190,9 @@ def eps_tables():
         eps, k = t(enei)
         key = name.replace(".dat", "")
         out[key + "_enei"], out[key + "_eps"], out[key + "_k"] = enei, np.asarray(eps), np.asarray(k)
+    for metal in ("gold", "silver", "aluminum"):
+        m = getattr(EpsDrude, metal)()
+        out["drude_" + metal] = np.array([m.eps0, m.wp, m.gammad])
     save("eps_tables.npz", **out)
 
 

@@ -83,3 +83,13 @@ def test_eps_tables_match_reference():
         EpsTable("gold.dat")(5000.0)
     with pytest.raises(FileNotFoundError):
         EpsTable("unobtainium.dat")
+
+
+def test_drude_presets_match_reference():
+    from conftest import golden
+    from mnpbem_b200.materials import EpsDrude
+    g = golden("eps_tables.npz")
+    for metal in ("gold", "silver", "aluminum"):
+        m = getattr(EpsDrude, metal)()
+        np.testing.assert_allclose([m.eps0, m.wp, m.gammad], g["drude_" + metal], rtol=1e-15)
+    assert EpsDrude.from_name("Au").wp == EpsDrude.gold().wp
