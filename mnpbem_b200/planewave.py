@@ -156,6 +156,30 @@ class PlaneWaveRet:
 
     __call__ = potential
 
+    def field(self, p, enei, inout=1):
+        """Electric and magnetic field of the plane wave at the faces whose
+        side ``inout`` (1 inside, 2 outside) touches the embedding medium:
+        e = exp(i k dir.r) pol, h = n_b dir x e (reference
+        planewave_ret.py:157-255).  Returns CompStruct(e, h), (n, 3[, npol])."""
+        if not np.allclose(np.sum(self.pol * self.dir, axis=1), 0):
+            raise ValueError("PlaneWaveRet: polarisation and direction must be orthogonal")
+        eps_val = p.eps[self.medium - 1](enei)[0]
+        nb = np.sqrt(eps_val)
+        k0 = 2 * np.pi / enei
+        k = k0 * nb
+        npol = self.pol.shape[0]
+        ind = np.flatnonzero(np.asarray(p.inout_faces)[:, inout - 1] == self.medium)
+        e = np.zeros((p.n, 3, npol), dtype=complex)
+        h = np.zeros((p.n, 3, npol), dtype=complex)
+        for i in range(npol):
+            if len(ind):
+                ph = np.exp(1j * k * p.pos[ind] @ self.dir[i]) / (1j * k0)
+                e[ind, :, i] = 1j * k0 * ph[:, None] * self.pol[i]
+            h[:, :, i] = nb * np.cross(np.tile(self.dir[i], (p.n, 1)), e[:, :, i])
+        if npol == 1:
+            e, h = e[:, :, 0], h[:, :, 0]
+        return CompStruct(p, enei, e=e, h=h)
+
     def rhs_device(self, p, enei, eps_mode, e1p, e2p, device="cuda"):
         """The BEM right-hand side of this plane wave directly on the device
         (8 n npol complex128, layout of BEMRet.rhs): potential() fused with the

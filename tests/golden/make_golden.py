@@ -32,6 +32,7 @@ input/output vectors that pin the oracle and the geometry module:
                           trisphere(144, 20) with tabulated gold (validation/08_iterative).
 * ``eps_tables.npz``    : eps and k of the reference EpsTable for each of its five tables,
                           and the parameters of its preset Drude metals.
+* ``planewave_field.npz`` : PlaneWaveRet.field of the reference on a small curved rod.
 
 Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only] [--meshes-only]
 """
@@ -196,6 +197,20 @@ def eps_tables():
     save("eps_tables.npz", **out)
 
 
+def planewave_field():
+    """PlaneWaveRet.field of the reference (x-pol along +z, z-pol along +x) on
+    the small curved rod trirod(12, 30, [9, 5, 5]) in water, inside and outside."""
+    from mnpbem.geometry import mesh_generators as mg
+    part = mg.trirod(12.0, 30.0, [9, 5, 5], interp="curv")
+    p = ComParticle([EpsConst(1.77), EpsDrude(*DRUDE_AU)], [part], [[2, 1]], 1, interp="curv")
+    exc = PlaneWaveRet(np.array([[1.0, 0, 0], [0, 0, 1.0]]), np.array([[0, 0, 1.0], [1.0, 0, 0]]))
+    out = {}
+    for inout in (1, 2):
+        f = exc.field(p, 600.0, inout=inout)
+        out["e%d" % inout], out["h%d" % inout] = f.e, f.h
+    save("planewave_field.npz", **out)
+
+
 def dimer_cfg1():
     p = _dimer(1444, 40.0, 1.0)
     t0 = time.time()
@@ -318,6 +333,7 @@ if __name__ == "__main__":
         matlab_rod()
         matlab_iter()
         eps_tables()
+        planewave_field()
         sys.exit(0)
     hmat_trees()
     if "--hmat-only" in sys.argv:
@@ -326,6 +342,7 @@ if __name__ == "__main__":
     matlab_rod()
     matlab_iter()
     eps_tables()
+    planewave_field()
     geom()
     refined_cfg0()
     matrices_s60()

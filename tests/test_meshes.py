@@ -95,3 +95,14 @@ def test_oracle_rod_matches_mnpbem17_and_reference():
         got = np.array([out["ext"][0], out["sca"][0], out["ext"][1], out["sca"][1]])
         assert np.max(np.abs(got - g["matlab"][i]) / np.abs(g["matlab"][i])) < 5e-10, i
         assert np.max(np.abs(got - g["python"][i]) / np.abs(g["python"][i])) < 1e-5, i
+
+
+def test_planewave_field_matches_reference():
+    from mnpbem_b200.planewave import PlaneWaveRet
+    g = golden("planewave_field.npz")
+    cp = shape_particle("rodbem")
+    exc = PlaneWaveRet([[1.0, 0, 0], [0, 0, 1.0]], [[0, 0, 1.0], [1.0, 0, 0]])
+    for inout in (1, 2):
+        f = exc.field(cp, 600.0, inout=inout)
+        np.testing.assert_allclose(f.e, g["e%d" % inout], rtol=1e-14, atol=1e-15)
+        np.testing.assert_allclose(f.h, g["h%d" % inout], rtol=1e-14, atol=1e-15)
