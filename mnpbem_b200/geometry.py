@@ -408,6 +408,21 @@ class Particle:
         self._norm()
         return self
 
+    def rot(self, angle, dir=None):
+        """Rotate by ``angle`` degrees about the axis ``dir`` (default z): the
+        vertices are multiplied from the right by expm(-angle K), K the
+        cross-product matrix of the unit axis (reference particle.py:778-818)."""
+        from scipy.linalg import expm
+        d = np.array([0.0, 0.0, 1.0]) if dir is None else np.asarray(dir, dtype=float)
+        d = d / np.linalg.norm(d)
+        K = np.array([[0.0, -d[2], d[1]], [d[2], 0.0, -d[0]], [-d[1], d[0], 0.0]])
+        R = expm(-(angle * np.pi / 180) * K)
+        self.verts = self.verts @ R
+        if self.verts2 is not None:
+            self.verts2 = self.verts2 @ R
+        self._norm()
+        return self
+
     def flipfaces(self):
         """Reverse the orientation of every face (reference particle.py:868-908)."""
         new = copy.deepcopy(self)
@@ -916,6 +931,44 @@ class ComParticle:
 
     def bradius(self):
         return np.hstack([q.bradius() for q in self.p])
+
+    # editing: applied to every particle, then the compound is rebuilt
+    # (reference comparticle.py:420-487)
+    def _each(self, method, *args, **kwargs):
+        self.p = [getattr(q, method)(*args, **kwargs) for q in self.p]
+        self._build()
+        return self
+
+    def shift(self, vec):
+        return self._each("shift", vec)
+
+    def scale(self, s):
+        return self._each("scale", s)
+
+    def rot(self, angle, dir=None):
+        return self._each("rot", angle, dir)
+
+    def flip(self, dir=0):
+        return self._each("flip", dir)
+
+    def flipfaces(self):
+        return self._each("flipfaces")
+
+    @property
+    def verts(self):
+        return self.pc.verts
+
+    @property
+    def faces(self):
+        return self.pc.faces
+
+    def ipart(self, ind):
+        """(particle index, local face index) of global face indices
+        (reference comparticle.py:987-1025)."""
+        ind = np.atleast_1d(np.asarray(ind, dtype=int))
+        off = self.offsets
+        part = np.searchsorted(off, ind, side="right") - 1
+        return part, ind - off[part]
 
     def __repr__(self):
         return "ComParticle(nparticles={}, nfaces={})".format(len(self.p), self.nfaces)

@@ -33,6 +33,7 @@ input/output vectors that pin the oracle and the geometry module:
 * ``eps_tables.npz``    : eps and k of the reference EpsTable for each of its five tables,
                           and the parameters of its preset Drude metals.
 * ``planewave_field.npz`` : PlaneWaveRet.field of the reference on a small curved rod.
+* ``editing.npz``       : Particle.rot and ComParticle shift / scale / rot / ipart of the reference.
 
 Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only] [--meshes-only]
 """
@@ -211,6 +212,25 @@ def planewave_field():
     save("planewave_field.npz", **out)
 
 
+def editing():
+    """Particle.rot and the ComParticle editing methods of the reference on
+    two curved spheres: rot(30 deg, [1, 1, 0]) of one, then the compound
+    shifted, scaled and rotated; ipart of a few global faces."""
+    a, b = trisphere(60, 10.0), trisphere(32, 6.0)
+    a.rot(30.0, [1.0, 1.0, 0.0])
+    b.shift([9.0, 0.0, 0.0])
+    p = ComParticle([EpsConst(1.0), EpsDrude(*DRUDE_AU)], [a, b], [[2, 1], [2, 1]], 1, 2, interp="curv")
+    out = {"rot_pos": a.pos, "rot_nvec": a.nvec, "rot_area": a.area}
+    p.shift([1.0, -2.0, 0.5])
+    p.scale(1.5)
+    p.rot(45.0, [0.0, 0.0, 1.0])
+    out.update(cp_pos=p.pos, cp_nvec=p.nvec, cp_area=p.area)
+    ind = np.array([0, 5, 115, 116, 150, 175])
+    pi, li = p.ipart(ind)
+    out.update(ipart_ind=ind, ipart_part=np.asarray(pi), ipart_local=np.asarray(li))
+    save("editing.npz", **out)
+
+
 def dimer_cfg1():
     p = _dimer(1444, 40.0, 1.0)
     t0 = time.time()
@@ -334,6 +354,7 @@ if __name__ == "__main__":
         matlab_iter()
         eps_tables()
         planewave_field()
+        editing()
         sys.exit(0)
     hmat_trees()
     if "--hmat-only" in sys.argv:
@@ -343,6 +364,7 @@ if __name__ == "__main__":
     matlab_iter()
     eps_tables()
     planewave_field()
+    editing()
     geom()
     refined_cfg0()
     matrices_s60()

@@ -93,3 +93,24 @@ def test_drude_presets_match_reference():
         m = getattr(EpsDrude, metal)()
         np.testing.assert_allclose([m.eps0, m.wp, m.gammad], g["drude_" + metal], rtol=1e-15)
     assert EpsDrude.from_name("Au").wp == EpsDrude.gold().wp
+
+
+def test_rot_and_compound_editing_match_reference():
+    from conftest import golden
+    from mnpbem_b200.geometry import ComParticle, trisphere
+    from mnpbem_b200.materials import EpsConst, EpsDrude
+    g = golden("editing.npz")
+    a, b = trisphere(60, 10.0), trisphere(32, 6.0)
+    a.rot(30.0, [1.0, 1.0, 0.0])
+    b.shift([9.0, 0.0, 0.0])
+    np.testing.assert_allclose(a.pos, g["rot_pos"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(a.nvec, g["rot_nvec"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(a.area, g["rot_area"], rtol=1e-13)
+    p = ComParticle([EpsConst(1.0), EpsDrude(9.84, 9.0, 0.067)], [a, b], [[2, 1], [2, 1]], 1, 2, interp="curv")
+    p.shift([1.0, -2.0, 0.5]).scale(1.5).rot(45.0, [0.0, 0.0, 1.0])
+    np.testing.assert_allclose(p.pos, g["cp_pos"], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(p.nvec, g["cp_nvec"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(p.area, g["cp_area"], rtol=1e-13)
+    part, local = p.ipart(g["ipart_ind"])
+    np.testing.assert_array_equal(part, g["ipart_part"])
+    np.testing.assert_array_equal(local, g["ipart_local"])
