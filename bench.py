@@ -37,6 +37,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "solves/s, 5768-face dimer: mixed+IR vs FP64 on 1 B200 at ext rel-err<=1e-8"
 GOLD_EXT_650 = None  # filled from tests/golden/dimer_cfg1.npz
+REF_MAX_SOLVES = 6   # timed CPU solves of the reference arm (each ~18 s)
 
 
 def parse():
@@ -180,9 +181,11 @@ def run_ours(args):
     clocks.start()
     n0 = L.bem200_launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    irs = []
     e0.record()
     for s in range(args.warmup, steps):
         device_step(*rhs[s])
+        irs.append(bem.last_ir)  # host values of the refinement (it synchronises once per sweep)
     e1.record()
     torch.cuda.synchronize()
     launches = L.bem200_launch_count() - n0
@@ -190,6 +193,10 @@ def run_ours(args):
     ck = clocks.stop()
     t_dev = maxover(e0.elapsed_time(e1) / 1e3)
     ir = bem.last_ir
+    ir_max = maxover(max(r[1] for r in irs)) if irs and irs[0] else None
+    if ir_max is not None and not ir_max <= bem.ir_tol:
+        raise RuntimeError("bench: a timed step left the refinement residual at {:.3e} > ir_tol {:.1e}"
+                           .format(ir_max, bem.ir_tol))
 
     # end to end through the public API (host excitation + transfers)
     barrier()
@@ -267,6 +274,8 @@ def run_ours(args):
             "engine": args.engine if args.precision == "mixed" else "simt",
             "ir_iterations": ir[0] if ir else None,
             "ir_relres": ir[1] if ir else None,
+            "ir_relres_max": ir_max,
+            "ir_methods": sorted({r[2] for r in irs}) if irs and irs[0] else None,
             "ext_650nm": ext650,
             "ext_rel_err_vs_reference_fp64": ext_err,
             "fp64_solves_per_s": round(fp64_rate, 4) if fp64_rate else None,
@@ -279,6 +288,14 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": ck,
         "roofline": roof,
+        "step_roofline": {
+            "flops_per_step": 32.0 * cp.n ** 3,
+            "flops_note": "32 N^3 real flops: 4 complex LUs, 2 N-RHS right solves, 1 inverse",
+            "achieved_tflops": round(32.0 * cp.n ** 3 * args.steps / t_dev / 1e12, 2),  # per GPU
+            "peak_tflops": roof["peak_sustained"] if roof else None,
+            "frac": round(32.0 * cp.n ** 3 * args.steps / t_dev / 1e12 / roof["peak_sustained"], 4) if roof else None,
+            "peak_source": roof["peak_sustained_source"] if roof else None,
+        },
         "cpu_baseline": cpu,
     }
     print(json.dumps(out), flush=True)
@@ -318,9 +335,11 @@ def roofline_gemm(dev):
     t = e0.elapsed_time(e1) / 1e3 / reps
     achieved = 8.0 * m * n * k / t / 1e12
     peak, src = 1590.0, "fallback (no MEASURED_PEAKS.json): earlier burst measurement on this pool"
+    peak_s, src_s = 1400.0, "fallback (no MEASURED_PEAKS.json): sustained figure under the power cap on this pool"
     try:
         mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak, src = float(mp["bf16_tflops"]), "measured bf16 burst"
+        peak_s, src_s = float(mp["bf16_tflops_sustained"]), "measured bf16 sustained"
     except Exception:
         pass
     # DRAM bytes (read + write) of one launch of this GEMM from an ncu capture of the same shape
@@ -329,7 +348,18 @@ def roofline_gemm(dev):
     return {"kernel": "tc::gemm_bf16x3_kernel (+ operand prep)", "bound": "tensor", "achieved": round(achieved, 2),
             "peak": peak, "peak_source": src, "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch",
-            "algorithmic_flops_per_launch": 8.0 * m * n * k, "shape": [m, n, k], "ms_per_launch": round(1e3 * t, 3)}
+            "algorithmic_flops_per_launch": 8.0 * m * n * k, "shape": [m, n, k], "ms_per_launch": round(1e3 * t, 3),
+            "peak_sustained": peak_s, "peak_sustained_source": src_s}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def cpu_baseline(cp):
@@ -341,7 +371,7 @@ def cpu_baseline(cp):
     t0 = time.time()
     ob.solve(650.0, POL, DIR)
     t = time.time() - t0
-    return {"value": round(1.0 / t, 5), "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+    return {"value": round(1.0 / t, 5), "unit": "solves/s", "cores": os.cpu_count(), "cpu": cpu_model(), "kind": "port",
             "sample": "1 full solve (Green matrices + Sigma/Delta LU build + solve + ext/sca) of the 5768-face "
                       "dimer at 650 nm, {:.1f} s".format(t)}
 
@@ -355,13 +385,17 @@ def run_reference(args):
     from oracle.pipeline import OracleBEM
     cp = dimer()
     ob = OracleBEM(cp)
-    for s in range(args.warmup):
+    # one CPU solve takes ~18 s: one untimed warm-up and at most REF_MAX_SOLVES
+    # timed solves keep the arm within a few minutes; the rate is per solve
+    warm = min(args.warmup, 1)
+    nsolve = max(1, min(args.steps, REF_MAX_SOLVES))
+    for s in range(warm):
         ob.solve(wavelength(s), POL, DIR)
     t0 = time.time()
-    for s in range(args.warmup, args.warmup + args.steps):
+    for s in range(warm, warm + nsolve):
         ob.solve(wavelength(s), POL, DIR)
     t = time.time() - t0
-    value = args.steps / t
+    value = nsolve / t
     out = {
         "metric": METRIC, "value": round(value, 5), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * t / args.steps, 1), "higher_is_better": True,
@@ -370,9 +404,10 @@ def run_reference(args):
         "config": {"workload": "5768-face Au sphere dimer, 2 nm gap, water, Drude Au, x-pol +z, lambda = 650 + 0.05 s nm",
                    "faces": cp.n, "parallelism": "host cores"},
         "impl": "reference",
-        "cpu_baseline": {"value": round(value, 5), "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": "{} full per-wavelength solves of the 5768-face dimer (CPU oracle, numpy/scipy "
-                                   "complex128)".format(args.steps)},
+        "cpu_baseline": {"value": round(value, 5), "unit": "solves/s", "cores": os.cpu_count(), "cpu": cpu_model(),
+                         "kind": "port",
+                         "sample": "{} timed full per-wavelength solves (after {} untimed) of the 5768-face dimer "
+                                   "(CPU oracle, numpy/scipy complex128, all host threads)".format(nsolve, warm)},
         "e2e": {"value": round(value, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)

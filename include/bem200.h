@@ -40,6 +40,7 @@ extern "C" {
 #define BEM200_ERR_SINGULAR 3     /* exactly singular pivot met in an LU */
 #define BEM200_ERR_UNSUPPORTED 4  /* configuration not implemented */
 #define BEM200_ERR_TIMEOUT 5      /* a bounded device-side wait gave up */
+#define BEM200_ERR_NOCONV 6       /* iterative refinement stopped above its tolerance */
 
 #define BEM200_C128 0 /* complex double, 16 bytes per element */
 #define BEM200_C64 1  /* complex float, 8 bytes per element */
@@ -164,9 +165,12 @@ int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* row
  * (or NULL) ws selects the single-stream schedule. */
 size_t bem200_getrf_workspace_size(int dtype, int engine, int n);
 /* B <- A^-1 B from the getrf factors (nrhs columns, row-major B).  scratch:
- * bem200_getrs_workspace_size bytes.  *status (device int, may be NULL) is set
- * to BEM200_ERR_TIMEOUT if a bounded device-side wait of the blocked
- * triangular solve gave up (the result is then invalid). */
+ * bem200_getrs_workspace_size bytes.  *status (device int) is set to
+ * BEM200_ERR_TIMEOUT if a bounded device-side wait of the blocked triangular
+ * solve (nrhs <= 16) gave up; the result is then invalid.  status may be NULL,
+ * but then such a timeout is recorded only in the scratch and goes
+ * unnoticed: callers that need to detect it pass a status int and read it
+ * after the stream completes. */
 size_t bem200_getrs_workspace_size(int dtype, int n, int nrhs);
 int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t ld, const int32_t* rowmap,
                  void* B, int64_t ldb, void* ws, size_t ws_bytes, void* scratch, int32_t* status,
@@ -181,8 +185,13 @@ int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t
  * until exit); sizes whose scratch (bem200_getrs_workspace_size) is larger
  * are rejected with BEM200_ERR_ARG.  The call allocates nothing.  The first
  * call on a device looks up the buffer's device address (host set-up); make
- * it before any stream capture.  All calls on a GPU share the buffer: calls
- * that overlap on the GPU race, so order them (one stream, or events). */
+ * it before any stream capture.  The address is kept per device ordinal for
+ * the life of the process: it belongs to the device's primary context and is
+ * stale after cudaDeviceReset or under another context on that device, so
+ * use this entry point only from the primary context and not across a
+ * device reset.  All calls on a GPU share the buffer: calls that overlap on
+ * the GPU race, so order them (one stream, or events).  As with
+ * bem200_getrs, pass status to detect a timed-out triangular solve. */
 #define BEM200_GETRS_NOALLOC_MAX_BYTES (4u << 20)
 int bem200_getrs_noalloc(int dtype, int n, int nrhs, const void* LU, int64_t ld, const int32_t* rowmap, void* B,
                          int64_t ldb, int32_t* status, void* stream);
@@ -231,7 +240,13 @@ int bem200_bem_apply(int n, int npol, const void* G1, const void* G2, const void
 /* Mixed-precision solve: x = M b with the complex64 factors in ws, then
  * x += M (b - A x) with the FP64 operator of G1..H2 (complex128) until
  * max|b - A x| <= tol max|b| or maxit sweeps.  *iters, *relres: HOST outputs.
- * This call synchronises the stream once per sweep to test convergence. */
+ * This call synchronises the stream once per sweep to test convergence.
+ * Returns BEM200_ERR_NOCONV when the refinement stops above tol: maxit
+ * sweeps reached, a residual that is not finite, or a sweep that does not
+ * reduce the residual (divergence).  W1, W2, *iters and *relres still hold
+ * the last iterate, so a caller can continue (GMRES-IR) or report it.
+ * BEM200_ERR_SINGULAR: the factors hold an exactly zero pivot;
+ * BEM200_ERR_TIMEOUT: a bounded device wait of a triangular solve gave up. */
 int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, const void* G2, const void* H1,
                         const void* H2, const void* b, int eps_per_face, const double* eps1, const double* eps2,
                         const double* nvec, double k0, double tol, int maxit, void* W1, void* W2, void* scratch,

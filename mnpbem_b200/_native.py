@@ -14,6 +14,11 @@ LIB_PATH = os.path.join(_HERE, "lib", "libbem200.so")
 C128 = 0
 C64 = 1
 
+# status codes (include/bem200.h)
+ERR_SINGULAR = 3
+ERR_TIMEOUT = 5
+ERR_NOCONV = 6
+
 _lib = None
 
 _vp = ctypes.c_void_p

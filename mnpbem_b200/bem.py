@@ -10,6 +10,12 @@ Everything per wavelength runs in libbem200 on the GPU:
   GEMMs (``engine='bf16x3'``; ``'simt'`` uses CUDA cores),
   then iterative refinement against the complex128 BEM operator until the
   max-norm residual drops below ``ir_tol`` times the right-hand side.
+  Refinement whose sweeps stop contracting (the contraction rate of
+  refinement is about cond(A) times the complex64 rounding error, so a slow
+  or diverging sweep is the condition estimate that the factors are not good
+  enough) continues as GMRES-IR: restarted GMRES on the FP64 operator,
+  right-preconditioned by the same complex64 factors (``gmres_ir=True``).
+  A solve that still misses ``ir_tol`` raises ``RuntimeError``.
 
 There is no CPU fallback: without a GPU or the library, construction raises.
 """
@@ -75,7 +81,8 @@ class BEMRet:
     name = "bemsolver"
     needs = {"sim": "ret"}
 
-    def __init__(self, p, enei=None, precision="fp64", engine="bf16x3", ir_tol=1e-12, ir_maxit=30, **options):
+    def __init__(self, p, enei=None, precision="fp64", engine="bf16x3", ir_tol=1e-12, ir_maxit=30, gmres_ir=True,
+                 gmres_maxit=200, **options):
         torch = _torch()
         if p is None:
             raise ValueError("BEMRet: 'p' must be a ComParticle (or compatible particle object), got None.")
@@ -93,6 +100,8 @@ class BEMRet:
         self.engine = engine if precision == "mixed" else "simt"
         self.ir_tol = float(ir_tol)
         self.ir_maxit = int(ir_maxit)
+        self.gmres_ir = bool(gmres_ir)
+        self.gmres_maxit = int(gmres_maxit)
         self.options = dict(options)
         self.enei = None
         self.dev = torch.device("cuda")
@@ -220,12 +229,63 @@ class BEMRet:
             it = ctypes.c_int32(0)
             rr = ctypes.c_double(0)
             G = self._G128
-            nat.call("bem200_bem_solve_ir", _ENGINES[self.engine], n, npol, nat.ptr(self._ws), nat.ptr(G[0]),
-                     nat.ptr(G[1]), nat.ptr(G[2]), nat.ptr(G[3]), nat.ptr(bt), self._eps_mode, self._e1p, self._e2p,
-                     nat.ptr(self._nvec), self.k, self.ir_tol, self.ir_maxit, nat.ptr(W1), nat.ptr(W2),
-                     nat.ptr(scratch), nat.ptr(self._gws), self._gws_bytes, ctypes.byref(it), ctypes.byref(rr), s)
-            self.last_ir = (int(it.value), float(rr.value))
+            st = L.bem200_bem_solve_ir(_ENGINES[self.engine], n, npol, nat.ptr(self._ws), nat.ptr(G[0]),
+                                       nat.ptr(G[1]), nat.ptr(G[2]), nat.ptr(G[3]), nat.ptr(bt), self._eps_mode,
+                                       self._e1p, self._e2p, nat.ptr(self._nvec), self.k, self.ir_tol, self.ir_maxit,
+                                       nat.ptr(W1), nat.ptr(W2), nat.ptr(scratch), nat.ptr(self._gws),
+                                       self._gws_bytes, ctypes.byref(it), ctypes.byref(rr), s)
+            self.last_ir = (int(it.value), float(rr.value), "ir")
+            if st == nat.ERR_NOCONV and self.gmres_ir:
+                W1, W2 = self._gmres_refine(bt, npol, W1, W2, int(it.value))
+            else:
+                nat.check(st, "bem200_bem_solve_ir")
         return W1, W2
+
+    def _gmres_refine(self, bt, npol, W1, W2, sweeps):
+        """GMRES-IR: continue a refinement that stopped contracting.  Solves
+        A d = b - A x0 by restarted GMRES on the FP64 operator, right
+        preconditioned by one solve with the complex64 factors, and returns
+        x0 + d.  The tolerance is ``ir_tol`` on the 2-norm residual relative to
+        ||b||; a miss raises RuntimeError."""
+        torch = _torch()
+        from .bem_iter import gmres
+        n = self.n
+        np_ = n * npol
+        L = nat.lib()
+        s = nat.stream_ptr()
+        G = self._G128
+        x0 = torch.cat([W1.reshape(-1), W2.reshape(-1)])
+        ascr = torch.empty(int(L.bem200_bem_apply_workspace_size(n, npol)), dtype=torch.uint8, device=self.dev)
+        pscr = torch.empty(int(L.bem200_bem_solve_workspace_size(1, n, npol)), dtype=torch.uint8, device=self.dev)
+
+        def apply_A(v, out, b=None):
+            nat.call("bem200_bem_apply", n, npol, nat.ptr(G[0]), nat.ptr(G[1]), nat.ptr(G[2]), nat.ptr(G[3]),
+                     self._eps_mode, self._e1p, self._e2p, nat.ptr(self._nvec), self.k, nat.ptr(v),
+                     ctypes.c_void_p(v.data_ptr() + 16 * 4 * np_), nat.ptr(b), nat.ptr(out), nat.ptr(ascr), s)
+
+        def apply_M(v, out):
+            nat.call("bem200_bem_precond", 1, _ENGINES[self.engine], n, npol, nat.ptr(self._ws), nat.ptr(v),
+                     self._eps_mode, self._e1p, self._e2p, nat.ptr(self._nvec), self.k, nat.ptr(out),
+                     nat.ptr(pscr), nat.ptr(self._gws), self._gws_bytes, s)
+
+        r0 = torch.empty_like(bt)
+        apply_A(x0, r0, b=bt)
+        bn = float(torch.linalg.vector_norm(bt))
+        rn = float(torch.linalg.vector_norm(r0))
+        if rn > self.ir_tol * bn:
+            d, res = gmres(apply_A, apply_M, r0, tol=self.ir_tol * bn / rn, maxit=self.gmres_maxit,
+                           restart=min(self.gmres_maxit, 50))
+            x0 += d
+            apply_A(x0, r0, b=bt)
+            rn = float(torch.linalg.vector_norm(r0))
+            self.last_ir = (sweeps, rn / bn, "gmres-ir", res.iter)
+        else:
+            self.last_ir = (sweeps, rn / bn, "gmres-ir", 0)
+        if not (rn <= self.ir_tol * bn):
+            raise RuntimeError("BEMRet: mixed-precision solve did not converge: {} refinement sweeps, then GMRES-IR "
+                               "left the residual at {:.3e} of the right-hand side (ir_tol {:.1e})"
+                               .format(sweeps, rn / bn, self.ir_tol))
+        return x0[:4 * np_].view(n, 4 * npol), x0[4 * np_:].view(n, 4 * npol)
 
     def check_status(self):
         """Raise if a factor met a zero pivot or a bounded device wait gave up."""

@@ -716,9 +716,11 @@ int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, c
   BEM_REQUIRE(bnorm > 0 && bnorm < 1e300, BEM200_ERR_ARG, "bem_solve_ir: right-hand side is zero or not finite");
   // x = M b  (mixed solve, scaled to unit magnitude)
   const double2* res = bb;
-  double rnorm = bnorm;
+  double rnorm = bnorm, prev = bnorm;
   int it = 0;
   bool first = true;
+  int outcome = BEM200_OK;
+  const BemState<float2> sv = state_view<float2>(n, ws);
   while (true) {
     double scale = 1.0 / rnorm;
     c128_to_c64_kernel<<<ceil_div(8 * np, 256), 256, 0, s>>>(8 * np, res, rhs32, scale);
@@ -735,22 +737,41 @@ int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, c
                         eps, nvec, k0, x, x + 4 * np, bb, r, opws)))
       return st;
     if ((st = absmax_host(s, 8 * np, r, red, &rnorm))) return st;
-    {
-      int hs = 0;
-      BEM_CUDA_CHECK(cudaMemcpyAsync(&hs, state_view<float2>(n, ws).status, sizeof(int), cudaMemcpyDeviceToHost, s));
-      BEM_CUDA_CHECK(cudaStreamSynchronize(s));
-      BEM_REQUIRE(hs == 0, BEM200_ERR_TIMEOUT, "bem_solve_ir: a bounded device wait gave up (status %d)", hs);
-    }
     ++it;
-    if (!(rnorm <= tol * bnorm) && !(rnorm < 1e300)) break;  // NaN / overflow: stop
-    if (rnorm <= tol * bnorm || it >= maxit) break;
+    {
+      int hs[2] = {0, 0};  // info (first zero pivot of the factors), status (bounded waits)
+      BEM_CUDA_CHECK(cudaMemcpyAsync(hs, sv.info, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      BEM_CUDA_CHECK(cudaStreamSynchronize(s));
+      BEM_REQUIRE(hs[0] == 0, BEM200_ERR_SINGULAR, "bem_solve_ir: the complex64 factors hold a zero pivot (%d)",
+                  hs[0]);
+      BEM_REQUIRE(hs[1] == 0, BEM200_ERR_TIMEOUT, "bem_solve_ir: a bounded device wait gave up (status %d)", hs[1]);
+    }
+    if (rnorm <= tol * bnorm) break;
+    if (!(rnorm < 1e300)) {  // NaN or overflow
+      outcome = BEM200_ERR_NOCONV;
+      set_error("bem_solve_ir: residual not finite after %d sweeps", it);
+      break;
+    }
+    if (it >= maxit) {
+      outcome = BEM200_ERR_NOCONV;
+      set_error("bem_solve_ir: %d sweeps left the residual at %.3e of the right-hand side (tol %.3e)", it,
+                rnorm / bnorm, tol);
+      break;
+    }
+    if (it > 1 && rnorm >= prev) {  // a sweep that does not contract: refinement diverges
+      outcome = BEM200_ERR_NOCONV;
+      set_error("bem_solve_ir: refinement stagnates at %.3e of the right-hand side after %d sweeps", rnorm / bnorm,
+                it);
+      break;
+    }
+    prev = rnorm;
     res = r;
   }
   *iters = it;
   *relres = rnorm / bnorm;
   BEM_CUDA_CHECK(cudaMemcpyAsync(W1, x, sizeof(double2) * 4 * np, cudaMemcpyDeviceToDevice, s));
   BEM_CUDA_CHECK(cudaMemcpyAsync(W2, x + 4 * np, sizeof(double2) * 4 * np, cudaMemcpyDeviceToDevice, s));
-  return BEM200_OK;
+  return outcome;
 }
 
 }  // extern "C"

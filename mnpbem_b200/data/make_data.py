@@ -72,4 +72,7 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MNPBEM_REFERENCE")
+    if not ref:
+        sys.exit("usage: python make_data.py <path of the reference checkout> (or set MNPBEM_REFERENCE)")
+    main(ref)

@@ -175,6 +175,9 @@ def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=4, engine
     else:
         workers = min(workers, len(enei))
     plan = sweep_plan([p.n for p in particles], len(enei), workers, schedule, units)
+    # the current device is per host thread: the workers adopt the caller's, on
+    # which every BEMRet below allocates its workspaces
+    dev = torch.cuda.current_device() if cuda else None
     t0 = time.perf_counter()
     solvers = [{m: solver_factory(particles[m], pol, dirs) for m, _ in plan[w]} for w in range(workers)]
     for per in solvers:
@@ -192,7 +195,9 @@ def solve_sweep(particles, enei, pol, dirs, precision="mixed", workers=4, engine
 
     def run(w):
         try:
-            stream = torch.cuda.Stream() if cuda else None
+            if cuda:
+                torch.cuda.set_device(dev)
+            stream = torch.cuda.Stream(device=dev) if cuda else None
             start.wait()
             tw = time.perf_counter()
             ctx = torch.cuda.stream(stream) if cuda else _nullcontext()
@@ -261,11 +266,23 @@ def solve_sweep_dist(particles, enei, pol, dirs, device=None, **kw):
     processing time first (cost n^3, ``partition_units``), every rank runs
     ``solve_sweep`` on its share, and two all-reduces (SUM of the zero-padded
     cross sections, MAX of the sweep time) give every rank the whole result.
-    No other exchange: the units are independent."""
+    No other exchange: the units are independent.
+
+    ``device`` holds the all-reduce buffers; by default the rank's GPU
+    (LOCAL_RANK) when the backend is NCCL, else the CPU.  With a GPU solver
+    the sweep runs on the current device, which is set to LOCAL_RANK when a
+    CUDA device is available and the caller has not chosen one."""
+    import os
+
     import torch
     import torch.distributed as dist
     world = dist.get_world_size() if dist.is_initialized() else 1
     rank = dist.get_rank() if dist.is_initialized() else 0
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if kw.get("solver_factory") is None and torch.cuda.is_available():
+        torch.cuda.set_device(local % torch.cuda.device_count())
+    if device is None and dist.is_initialized() and dist.get_backend() == "nccl":
+        device = torch.device("cuda", local % torch.cuda.device_count())
     enei = np.asarray(enei, dtype=float).ravel()
     share = partition_units([p.n for p in particles], len(enei), world)[rank]
     r = solve_sweep(particles, enei, pol, dirs, units=share, **kw)

@@ -13,7 +13,9 @@ import os
 import sys
 import types
 
-REFERENCE_ROOT = os.environ.get("MNPBEM_REFERENCE", "/root/reference")
+REFERENCE_ROOT = os.environ.get("MNPBEM_REFERENCE")
+if not REFERENCE_ROOT:
+    raise RuntimeError("set MNPBEM_REFERENCE to the path of the reference checkout to generate fixtures")
 _STUB_ROOTS = ("matplotlib", "mpl_toolkits", "tqdm")
 
 

@@ -35,7 +35,8 @@ input/output vectors that pin the oracle and the geometry module:
 * ``planewave_field.npz`` : PlaneWaveRet.field of the reference on a small curved rod.
 * ``editing.npz``       : Particle.rot and ComParticle shift / scale / rot / ipart of the reference.
 
-Usage:  python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only] [--meshes-only]
+Usage:  MNPBEM_REFERENCE=<reference checkout> python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only]
+        [--meshes-only]
 """
 import os
 import sys
