@@ -141,6 +141,50 @@ int bem200_green_assemble_dk(int n, int npart, const int32_t* pid, const int32_t
                              int order, const double* g, const double* fn, void* G1, void* G2, void* H1, void* H2,
                              int64_t ld, void* stream);
 
+/* ------------------------------------------------------------------ (f4)
+ * Cartesian derivatives of the Green function and the potentials / fields of
+ * a solution at the faces.  blk, blk0, blk1: (npart x npart) int32 material
+ * index (1-based, 0 = not connected) of one region pair per particle block,
+ * i.e. con[i][j] of the reference; kmat_host as in bem200_green_assemble.
+ *
+ * bem200_green_assemble_cart: out (n, 3, n) complex128, out[i][c][j] =
+ *   Gp_c = (r_c)(ik - 1/d) / d^2 area_j e^{ikd} (refined pairs:
+ *   sum_q f[e][c][q] (ik)^q e^{ikd}), plus (hkey 1: H1p) 2 pi n_i or (hkey 2:
+ *   H2p) -2 pi n_i on the diagonal of self blocks (hkey 0: Gp).  f: the
+ *   (nref, 3, order+1) coefficients of bem200_refine_integrals after the
+ *   closed-surface correction.  Replaces CompGreenRet.eval with keys Gp, H1p,
+ *   H2p (mnpbem/greenfun/compgreen_ret.py:811-858,
+ *   mnpbem/greenfun/greenret_refined.py:812-864).
+ *
+ * bem200_green_potential: phi = G0 sig1 + G1 sig2, phip = H0 sig1 + H1 sig2,
+ *   a = G0 h1 + G1 h2, ap = H0 h1 + H1 h2, with G0, H0 of region pair blk0 and
+ *   G1, H1 of blk1, H the key H1 (hkey 1) or H2 (hkey 2).  sig1, sig2, phi,
+ *   phip: (n, npol); h1, h2, a, ap: (n, 3, npol), complex128, device.  The
+ *   matrices are never stored: entries are computed on the fly.  ref_row_ptr
+ *   (n + 1, int64, NULL = none), ref_col, g, fn: refinement tables in CSR
+ *   form.  Replaces CompGreenRet.potential
+ *   (mnpbem/greenfun/compgreen_ret.py:976-1038).
+ *
+ * bem200_green_field: e = i k0 (G0 h1 + G1 h2) - Hp0 sig1 - Hp1 sig2,
+ *   h = Hp0 x h1 + Hp1 x h2, Hp the key H1p (hkey 1) or H2p (hkey 2); e, h
+ *   (n, 3, npol).  f: (nref, 3, order+1).  Replaces CompGreenRet.field
+ *   (mnpbem/greenfun/compgreen_ret.py:912-974).  Both products support
+ *   n <= 98304 faces. */
+int bem200_green_assemble_cart(int n, int npart, const int32_t* pid, const int32_t* blk, int nmat,
+                               const double* kmat_host, const double* pos, const double* nvec, const double* area,
+                               int64_t nref, const int32_t* ref_row, const int32_t* ref_col, int order,
+                               const double* f, int hkey, void* out, void* stream);
+int bem200_green_potential(int n, int npart, const int32_t* pid, const int32_t* blk0, const int32_t* blk1, int nmat,
+                           const double* kmat_host, const double* pos, const double* nvec, const double* area,
+                           const int64_t* ref_row_ptr, const int32_t* ref_col, int order, const double* g,
+                           const double* fn, int hkey, int npol, const void* sig1, const void* sig2, const void* h1,
+                           const void* h2, void* phi, void* phip, void* a, void* ap, void* stream);
+int bem200_green_field(int n, int npart, const int32_t* pid, const int32_t* blk0, const int32_t* blk1, int nmat,
+                       const double* kmat_host, const double* pos, const double* nvec, const double* area,
+                       const int64_t* ref_row_ptr, const int32_t* ref_col, int order, const double* g, const double* f,
+                       int hkey, double k0, int npol, const void* sig1, const void* sig2, const void* h1,
+                       const void* h2, void* e, void* h, void* stream);
+
 /* ------------------------------------------------------------- dense LA
  * Building blocks of the dense BEM (reference: the LU / lu_solve / matmul
  * calls of mnpbem/bem/bem_ret.py:437-523, dispatched through

@@ -47,6 +47,14 @@ _SIGS = {
     "bem200_green_assemble_dk": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp,
                                                 ctypes.c_int, _vp, _vp, _vp, _i64, _vp, _vp, ctypes.c_int, _vp, _vp,
                                                 _vp, _vp, _vp, _vp, _i64, _vp]),
+    "bem200_green_assemble_cart": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, _vp,
+                                                  _vp, _i64, _vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp]),
+    "bem200_green_potential": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp,
+                                              _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp,
+                                              _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "bem200_green_field": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                          _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _dbl, ctypes.c_int, _vp, _vp,
+                                          _vp, _vp, _vp, _vp, _vp]),
     "bem200_gemm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                    _i64, _vp, _i64, _vp, _vp, _i64, _vp, _sz, _vp]),
     "bem200_gemm_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),

@@ -339,11 +339,17 @@ class BEMRet:
         return self
 
     def potential(self, sig, inout=2):
-        """Potentials of a solution at the faces (reference bem_ret.py:1833,
-        via CompGreenRet.potential): not provided by this library."""
-        raise NotImplementedError("BEMRet.potential: surface potentials of a solution are not implemented on the GPU")
+        """Potentials and surface derivatives of a solution inside (inout=1) or
+        outside (inout=2, default) of the particle surface (reference
+        bem_ret.py:1833-1859, delegating to CompGreenRet.potential): phi, phip,
+        a, ap computed on the GPU without storing the Green matrices (so no
+        factorisation at sig.enei is needed)."""
+        return self.g.potential(sig, inout)
 
     def field(self, sig, inout=2):
-        """Fields of a solution (reference bem_ret.py:1861, via CompGreenRet.field
-        and the Cartesian-derivative Green functions): not provided."""
-        raise NotImplementedError("BEMRet.field: fields of a solution are not implemented on the GPU")
+        """Electric and magnetic fields of a solution inside (inout=1) or
+        outside (inout=2, default) of the particle surface (reference
+        bem_ret.py:1861-1895, delegating to CompGreenRet.field with the
+        Cartesian-derivative Green functions H1p / H2p), computed on the GPU
+        without storing the Green matrices."""
+        return self.g.field(sig, inout)

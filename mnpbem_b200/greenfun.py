@@ -10,6 +10,9 @@ fused kernel pass.  All work runs in libbem200 kernels:
 * polar / 28-point refinement integrals             -> bem200_refine_integrals
 * closed-surface (Fuchs-Liu) diagonal correction    -> bem200_closed_correction
 * far field + refined overlay + e^{ikd}             -> bem200_green_assemble
+* Cartesian derivatives Gp, H1p, H2p                -> bem200_green_assemble_cart
+* potentials / fields of a solution at the faces    -> bem200_green_potential / _field
+  (entries computed on the fly, no n x n matrix stored)
 """
 import ctypes
 
@@ -181,16 +184,20 @@ class CompGreenRet:
     def eval(self, i, j, key, enei, ind=None, as_tensor=False):
         """One region-pair matrix (reference CompGreenRet.eval, compgreen_ret.py:507).
 
-        Returns a host numpy array (or the device tensor when ``as_tensor``),
-        or the int 0 when region i of no particle connects to region j.
+        Keys G, F, H1, H2 give (n, n) matrices; Gp, H1p, H2p the Cartesian
+        derivatives as (n, 3, n) arrays (reference layout).  Returns a host
+        numpy array (or the device tensor when ``as_tensor``), or the int 0
+        when region i of no particle connects to region j.
         """
         if ind is not None:
             raise NotImplementedError("CompGreenRet.eval: element selection (ind) is not supported")
-        if key not in ("G", "F", "H1", "H2"):
-            raise NotImplementedError("CompGreenRet.eval: key {!r} is not supported".format(key))
+        if key not in ("G", "F", "H1", "H2", "Gp", "H1p", "H2p"):
+            raise ValueError("Unknown key: {}".format(key))
         if not np.any(self.con[i][j] > 0):
             return 0
-        if key == "G":
+        if key in ("Gp", "H1p", "H2p"):
+            M = self.eval_cart(i, j, key, enei)
+        elif key == "G":
             M = self.assemble(enei, [(i, j), None, None, None], outputs=(True, False, False, False))[0]
         elif key in ("H1", "F"):
             M = self.assemble(enei, [(i, j), None, None, None], outputs=(False, False, True, False))[2]
@@ -199,6 +206,102 @@ class CompGreenRet:
         else:
             M = self.assemble(enei, [None, None, (i, j), None], outputs=(False, False, False, True))[3]
         return M if as_tensor else M.cpu().numpy()
+
+    def _kmat(self, enei):
+        ks = self.wavenumbers(enei)
+        return len(ks), (ctypes.c_double * (2 * len(ks)))(*[v for k in ks for v in (k.real, k.imag)])
+
+    def _con_table(self, i, j):
+        torch = _torch()
+        return torch.as_tensor(np.ascontiguousarray(self.con[i][j], dtype=np.int32).reshape(-1), device=self.device)
+
+    def eval_cart(self, i, j, key, enei):
+        """Gp, H1p or H2p of region pair (i, j) as an (n, 3, n) complex128
+        device tensor (reference greenret_refined.py:812-864, assembled per
+        particle block as compgreen_ret.py:811-858 does)."""
+        torch = _torch()
+        n = self.n
+        nmat, kmat = self._kmat(enei)
+        out = torch.empty((n, 3, n), dtype=torch.complex128, device=self.device)
+        r = self.refined
+        blk = self._con_table(i, j)
+        nat.call("bem200_green_assemble_cart", n, self.npart, nat.ptr(self.pid), nat.ptr(blk), nmat,
+                 ctypes.cast(kmat, ctypes.c_void_p), nat.ptr(self.pos), nat.ptr(self.nvec), nat.ptr(self.area),
+                 r.nref, nat.ptr(r.row), nat.ptr(r.col), self.order, nat.ptr(r.f),
+                 {"Gp": 0, "H1p": 1, "H2p": 2}[key], nat.ptr(out), nat.stream_ptr())
+        return out
+
+    def _solution_device(self, sig):
+        """sig1, sig2 (n, p) and h1, h2 (n, 3, p) of a solution as complex128
+        device tensors, and p."""
+        torch = _torch()
+        n = self.n
+        vals = [np.asarray(getattr(sig, k)) for k in ("sig1", "sig2", "h1", "h2")]
+        npol = 1 if vals[0].ndim == 1 else vals[0].shape[1]
+        out = []
+        for k, v in enumerate(vals):
+            shape = (n, npol) if k < 2 else (n, 3, npol)
+            out.append(torch.as_tensor(np.ascontiguousarray(v.reshape(shape)), dtype=torch.complex128,
+                                       device=self.device))
+        return out, npol
+
+    def _apply(self, sig, inout, field):
+        torch = _torch()
+        if inout not in (1, 2):
+            raise ValueError("inout must be 1 (inside) or 2 (outside)")
+        n = self.n
+        r = self.refined
+        reg = min(inout - 1, len(self.con) - 1)
+        (s1, s2, h1, h2), npol = self._solution_device(sig)
+        nmat, kmat = self._kmat(sig.enei)
+        blk0, blk1 = self._con_table(reg, 0), self._con_table(reg, 1)
+        cdt = dict(dtype=torch.complex128, device=self.device)
+        common = [n, self.npart, nat.ptr(self.pid), nat.ptr(blk0), nat.ptr(blk1), nmat,
+                  ctypes.cast(kmat, ctypes.c_void_p), nat.ptr(self.pos), nat.ptr(self.nvec), nat.ptr(self.area),
+                  nat.ptr(r.row_ptr) if r.nref > 0 else None, nat.ptr(r.col), self.order, nat.ptr(r.g)]
+        if field:
+            e = torch.empty((n, 3, npol), **cdt)
+            hh = torch.empty((n, 3, npol), **cdt)
+            nat.call("bem200_green_field", *common, nat.ptr(r.f), inout, 2 * np.pi / sig.enei, npol, nat.ptr(s1),
+                     nat.ptr(s2), nat.ptr(h1), nat.ptr(h2), nat.ptr(e), nat.ptr(hh), nat.stream_ptr())
+            return [e, hh], npol
+        phi = torch.empty((n, npol), **cdt)
+        phip = torch.empty((n, npol), **cdt)
+        a = torch.empty((n, 3, npol), **cdt)
+        ap = torch.empty((n, 3, npol), **cdt)
+        nat.call("bem200_green_potential", *common, nat.ptr(r.fn), inout, npol, nat.ptr(s1), nat.ptr(s2),
+                 nat.ptr(h1), nat.ptr(h2), nat.ptr(phi), nat.ptr(phip), nat.ptr(a), nat.ptr(ap), nat.stream_ptr())
+        return [phi, phip, a, ap], npol
+
+    def potential(self, sig, inout=1):
+        """Potentials and surface derivatives of solution ``sig`` inside
+        (inout=1) or outside (inout=2) of the surface (reference
+        CompGreenRet.potential, compgreen_ret.py:976-1038):
+        phi = G sig1 + G sig2, phip = H sig1 + H sig2, a = G h1 + G h2,
+        ap = H h1 + H h2 with the Green functions of region pairs
+        (inout, 1) and (inout, 2) and H = H1 (inside) or H2 (outside).
+        Returns a CompStruct with phi1, phi1p, a1, a1p (or phi2 ...)."""
+        from .planewave import CompStruct
+        (phi, phip, a, ap), npol = self._apply(sig, inout, field=False)
+        phi, phip, a, ap = [t.cpu().numpy() for t in (phi, phip, a, ap)]
+        if npol == 1:
+            phi, phip, a, ap = phi[:, 0], phip[:, 0], a[:, :, 0], ap[:, :, 0]
+        sfx = str(inout)
+        return CompStruct(self.p1, sig.enei, **{"phi" + sfx: phi, "phi" + sfx + "p": phip, "a" + sfx: a,
+                                               "a" + sfx + "p": ap})
+
+    def field(self, sig, inout=1):
+        """Electric and magnetic fields of solution ``sig`` at the faces, inside
+        (inout=1) or outside (inout=2) (reference CompGreenRet.field,
+        compgreen_ret.py:912-974): e = i k (G h1 + G h2) - Hp sig1 - Hp sig2,
+        h = Hp x h1 + Hp x h2 with Hp = H1p (inside) or H2p (outside).
+        Returns a CompStruct with e and h ((n, 3) or (n, 3, npol))."""
+        from .planewave import CompStruct
+        (e, h), npol = self._apply(sig, inout, field=True)
+        e, h = e.cpu().numpy(), h.cpu().numpy()
+        if npol == 1:
+            e, h = e[:, :, 0], h[:, :, 0]
+        return CompStruct(self.p1, sig.enei, e=e, h=h)
 
     def _sub_diag(self, M, rp, val):
         torch = _torch()

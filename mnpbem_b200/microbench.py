@@ -9,6 +9,7 @@
     python -m mnpbem_b200.microbench large [--side 3 | --shape cube] [--hmatrix] [--tol 1e-8]
     python -m mnpbem_b200.microbench sweep [--seed 0] [--nlambda 128] [--workers 4] [--schedule interleave|mesh]
     python -m mnpbem_b200.microbench shape [--nlambda 5] [--ndir 32] [--check 4] [--precision mixed]
+    python -m mnpbem_b200.microbench peaks [--m 8192] [--reps 5]
 
 ``step`` runs whole per-wavelength solves (assembly + init + solve) of the
 sphere dimer (two trisphere(faces) spheres, 2 nm gap, water, Drude gold,
@@ -341,10 +342,39 @@ def case_shape(a):
             "max_mem_GB": torch.cuda.max_memory_allocated() / 1e9}
 
 
+def case_peaks(a):
+    """Reference pipe rates of this GPU, from cuBLAS through torch.matmul
+    (library GEMMs used only as a yardstick): FP64 (DGEMM, ZGEMM), FP32
+    without and with TF32, and dense bf16; m = n = k = a.m (default 8192),
+    CUDA events over a.reps launches after one warm-up.  Complex GEMMs count
+    8 real flops per multiply-add."""
+    import torch
+    n = a.m if a.m != 5768 else 8192
+    out = {"case": "peaks", "size": n}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    try:
+        for name, dt, tf32, cx in (("fp64", torch.float64, False, False), ("c128", torch.complex128, False, True),
+                                   ("fp32", torch.float32, False, False), ("tf32", torch.float32, True, False),
+                                   ("bf16", torch.bfloat16, False, False)):
+            torch.backends.cuda.matmul.allow_tf32 = tf32
+            m = n // 2 if cx else n
+            A = torch.randn(m, m, dtype=dt, device="cuda")
+            B = torch.randn(m, m, dtype=dt, device="cuda")
+            torch.matmul(A, B)
+            ms = _timed(lambda: torch.matmul(A, B), a.reps)
+            flops = (8.0 if cx else 2.0) * m ** 3
+            out[name + "_tflops"] = round(flops / ms / 1e9, 2)
+            del A, B
+            torch.cuda.empty_cache()
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter", "large", "sweep",
-                                           "shape"])
+                                           "shape", "peaks"])
     ap.add_argument("--faces", type=int, default=1444)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--engine", type=int, default=1)
@@ -380,7 +410,7 @@ def main(argv=None):
         a.engine = {0: "simt", 1: "bf16x3"}[a.engine]
     out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf, "hmat": case_hmat,
            "iter": case_iter, "large": case_large, "sweep": case_sweep,
-           "shape": case_shape}[a.case](a)
+           "shape": case_shape, "peaks": case_peaks}[a.case](a)
     print(json.dumps(out), flush=True)
 
 

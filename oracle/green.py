@@ -247,8 +247,9 @@ def refine_all(cp, order=5):
 def green_block(pa, pb, blk, k, key, same):
     """G or F (cart derivative projected on n) of one particle block at complex
     wavenumber k: far field from centroids, refined entries overwritten by
-    sum_n c_n (ik)^n, then multiplied by exp(ikd).
-    Reference: mnpbem/greenfun/greenret_refined.py:654-810 (MATLAB eval1.m:18-153).
+    sum_n c_n (ik)^n, then multiplied by exp(ikd).  Keys Gp, H1p, H2p give the
+    Cartesian derivative as an (na, 3, nb) array.
+    Reference: mnpbem/greenfun/greenret_refined.py:654-864 (MATLAB eval1.m:18-153).
     """
     x = pa.pos[:, 0:1] - pb.pos[:, 0]
     y = pa.pos[:, 1:2] - pb.pos[:, 1]
@@ -257,6 +258,18 @@ def green_block(pa, pb, blk, k, key, same):
     if same:
         np.fill_diagonal(d, EPS)
     ikp = np.array([(1j * k) ** n for n in range(blk.g.shape[1])])
+    if key in ("Gp", "H1p", "H2p"):
+        aux = (1j * k - 1.0 / d) / d ** 2 * pb.area[None, :]
+        comps = []
+        for c, r in enumerate((x, y, z)):
+            M = aux * r + 0j
+            M[blk.rows, blk.cols] = blk.f[:, c, :] @ ikp
+            comps.append(M * np.exp(1j * k * d))
+        Gp = np.stack(comps, axis=1)
+        if same and key != "Gp":
+            idx = np.arange(pa.n)
+            Gp[idx, :, idx] += (2 * np.pi if key == "H1p" else -2 * np.pi) * pa.nvec
+        return Gp
     if key == "G":
         M = (1.0 / d) * pb.area[None, :] + 0j
         M[blk.rows, blk.cols] = blk.g @ ikp
@@ -280,13 +293,14 @@ def green_region(cp, blocks, i, j, key, enei):
     ks = [m(enei)[1] for m in cp.eps]
     off = cp.offsets
     M = None
+    cart = key in ("Gp", "H1p", "H2p")
     for a in range(len(cp.p)):
         for b in range(len(cp.p)):
             if con[a, b] > 0:
                 if M is None:
-                    M = np.zeros((cp.n, cp.n), dtype=complex)
+                    M = np.zeros((cp.n, 3, cp.n) if cart else (cp.n, cp.n), dtype=complex)
                 kb = complex(np.asarray(ks[con[a, b] - 1]).ravel()[0])
-                M[off[a]:off[a + 1], off[b]:off[b + 1]] = green_block(
+                M[off[a]:off[a + 1], ..., off[b]:off[b + 1]] = green_block(
                     cp.p[a], cp.p[b], blocks[a][b], kb, key, a == b)
     if M is None or np.all(M == 0):
         return 0
@@ -307,3 +321,55 @@ def bem_matrices(cp, blocks, enei):
     H1 = sub(green_region(cp, blocks, 0, 0, "H1", enei), green_region(cp, blocks, 1, 0, "H1", enei))
     H2 = sub(green_region(cp, blocks, 1, 1, "H2", enei), green_region(cp, blocks, 0, 1, "H2", enei))
     return G1, G2, H1, H2
+
+
+# --------------------------------------------------------------------------- f4
+def _mm(M, x):
+    """Matrix (n, n) or derivative (n, 3, n) times a vector field over the
+    last axis of M (reference CompGreenRet._matmul, compgreen_ret.py:1040-1098).
+    The int 0 (no connected block) gives 0."""
+    if isinstance(M, int):
+        return 0
+    return np.tensordot(M, x, axes=([M.ndim - 1], [0]))
+
+
+def _cross(Gp, h):
+    """Gp x h with Gp (n, 3, n) and h (n, 3, p) (reference CompGreenRet._cross,
+    compgreen_ret.py:1100-1136)."""
+    if isinstance(Gp, int):
+        return 0
+    out = np.zeros((Gp.shape[0], 3, h.shape[2]), dtype=complex)
+    for c in range(3):
+        c1, c2 = (c + 1) % 3, (c + 2) % 3
+        out[:, c] = Gp[:, c1, :] @ h[:, c2, :] - Gp[:, c2, :] @ h[:, c1, :]
+    return out
+
+
+def potential(cp, blocks, sig1, sig2, h1, h2, enei, inout):
+    """Potentials and surface derivatives of a solution inside (inout 1) or
+    outside (inout 2): phi, phip (n, p), a, ap (n, 3, p).
+    Reference: CompGreenRet.potential, mnpbem/greenfun/compgreen_ret.py:976-1038."""
+    r = inout - 1
+    hk = "H1" if inout == 1 else "H2"
+    G1, G2 = green_region(cp, blocks, r, 0, "G", enei), green_region(cp, blocks, r, 1, "G", enei)
+    H1, H2 = green_region(cp, blocks, r, 0, hk, enei), green_region(cp, blocks, r, 1, hk, enei)
+    phi = _mm(G1, sig1) + _mm(G2, sig2)
+    phip = _mm(H1, sig1) + _mm(H2, sig2)
+    a = _mm(G1, h1) + _mm(G2, h2)
+    ap = _mm(H1, h1) + _mm(H2, h2)
+    return phi, phip, a, ap
+
+
+def field(cp, blocks, sig1, sig2, h1, h2, enei, inout):
+    """Electric and magnetic fields at the faces, inside (inout 1) or outside
+    (inout 2): e, h (n, 3, p).
+    Reference: CompGreenRet.field, mnpbem/greenfun/compgreen_ret.py:912-974."""
+    r = inout - 1
+    k = 2 * np.pi / enei
+    hk = "H1p" if inout == 1 else "H2p"
+    G1, G2 = green_region(cp, blocks, r, 0, "G", enei), green_region(cp, blocks, r, 1, "G", enei)
+    e = 1j * k * (_mm(G1, h1) + _mm(G2, h2))
+    P1, P2 = green_region(cp, blocks, r, 0, hk, enei), green_region(cp, blocks, r, 1, hk, enei)
+    e = e - _mm(P1, sig1) - _mm(P2, sig2)
+    h = _cross(P1, h1) + _cross(P2, h2)
+    return e, h

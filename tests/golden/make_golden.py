@@ -34,9 +34,12 @@ input/output vectors that pin the oracle and the geometry module:
                           and the parameters of its preset Drude metals.
 * ``planewave_field.npz`` : PlaneWaveRet.field of the reference on a small curved rod.
 * ``editing.npz``       : Particle.rot and ComParticle shift / scale / rot / ipart of the reference.
+* ``field_potential.npz`` : BEMRet.potential / .field inside and outside and slices of the
+                          Cartesian-derivative Green functions (Gp, H1p, H2p) of the small dimer
+                          (two polarisations) and the vacuum sphere.
 
 Usage:  MNPBEM_REFERENCE=<reference checkout> python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only]
-        [--meshes-only]
+        [--meshes-only] [--field-only]
 """
 import os
 import sys
@@ -249,6 +252,42 @@ def dimer_cfg1():
          sig2_head=sig.sig2[:64], ctor_s=t1 - t0, solve_s=t2 - t1)
 
 
+def field_potential():
+    """BEMRet.potential / BEMRet.field (reference bem_ret.py:1833-1895 via
+    CompGreenRet.potential / .field, compgreen_ret.py:912-1038) inside and
+    outside, for the reference's own solutions: the small dimer at 620 nm with
+    two polarisations and the vacuum sphere at 600 nm; plus slices and sums of
+    the Cartesian-derivative Green functions (eval keys Gp, H1p, H2p)."""
+    out = {}
+    cases = (("dimer", _dimer(144, 10.0, 1.0), 620.0, np.array([[1.0, 0, 0], [0, 1.0, 0]]),
+              np.array([[0, 0, 1.0], [0, 0, 1.0]])),
+             ("sphere", ComParticle([EpsConst(1.0), EpsDrude(*DRUDE_AU)], [trisphere(144, 20)], [[2, 1]], 1,
+                                    interp="curv"), 600.0, POL, DIR))
+    for tag, p, enei, pol, dirs in cases:
+        bem = BEMRet(p)
+        exc = PlaneWaveRet(pol, dirs)
+        sig, bem = bem.solve(exc.potential(p, enei))
+        out[tag + "_enei"] = enei
+        for k in ("sig1", "sig2", "h1", "h2"):
+            out[tag + "_" + k] = getattr(sig, k)
+        for io in (1, 2):
+            pot = bem.potential(sig, io)
+            for k in ("phi", "phip", "a", "ap"):
+                name = k[:-1] + str(io) + "p" if k.endswith("p") and k != "phi" else k + str(io)
+                if k == "phip":
+                    name = "phi{}p".format(io)
+                out["{}_pot{}_{}".format(tag, io, k)] = getattr(pot, name)
+            f = bem.field(sig, io)
+            out["{}_field{}_e".format(tag, io)] = f.e
+            out["{}_field{}_h".format(tag, io)] = f.h
+        for (i, j, key) in ((0, 0, "H1p"), (1, 1, "H2p"), (1, 1, "Gp"), (0, 0, "Gp")):
+            M = bem.g.eval(i, j, key, enei)
+            nm = "{}_{}{}{}".format(tag, key, i, j)
+            out[nm + "_rows"] = np.asarray(M)[:8]
+            out[nm + "_abssum"] = np.sum(np.abs(M))
+    save("field_potential.npz", **out)
+
+
 def hmat_trees():
     """Cluster trees, block partitions and ACA ranks of the reference H-matrix
     (mnpbem/greenfun/clustertree.py, hmatrix.py) for the sphere (cleaf 32,
@@ -349,6 +388,9 @@ def meshes():
 
 
 if __name__ == "__main__":
+    if "--field-only" in sys.argv:
+        field_potential()
+        sys.exit(0)
     if "--meshes-only" in sys.argv:
         meshes()
         matlab_rod()
@@ -372,5 +414,6 @@ if __name__ == "__main__":
     spectrum_cfg0()
     dimer_small()
     matlab_cfg0()
+    field_potential()
     if "--skip-cfg1" not in sys.argv:
         dimer_cfg1()

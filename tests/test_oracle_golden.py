@@ -108,3 +108,34 @@ def test_oracle_iterative_matches_mnpbem17():
         ext = off.extinction(cp, s1[:, None], s2[:, None], h1[:, :, None], h2[:, :, None], enei, POL, DIR)[0]
         assert abs(ext - g["ext_iter"][i]) / g["ext_iter"][i] < 1e-7, (i, ext, g["ext_iter"][i])
         assert abs(g["ext_iter"][i] - g["ext_direct"][i]) / g["ext_direct"][i] < 1e-9
+
+
+def _fixture_solution(g, tag):
+    s = [g[tag + "_" + k] for k in ("sig1", "sig2", "h1", "h2")]
+    if s[0].ndim == 1:
+        s = [s[0][:, None], s[1][:, None], s[2][:, :, None], s[3][:, :, None]]
+    return s
+
+
+@pytest.mark.parametrize("tag,mk", [("dimer", dimer), ("sphere", sphere)])
+def test_potential_field_and_cart_derivatives(tag, mk):
+    """Oracle CompGreenRet.potential / .field (inside and outside) and the
+    Gp / H1p / H2p Green functions against the reference's own BEMRet.potential
+    / .field and eval on its solutions (field_potential.npz)."""
+    g = golden("field_potential.npz")
+    cp = mk()
+    ob = OracleBEM(cp)
+    enei = float(g[tag + "_enei"])
+    s = _fixture_solution(g, tag)
+    for io in (1, 2):
+        for k, v in zip(("phi", "phip", "a", "ap"), og.potential(cp, ob.blocks, *s, enei, io)):
+            ref = g["{}_pot{}_{}".format(tag, io, k)]
+            assert rel(np.asarray(v).reshape(ref.shape), ref) < 1e-13, (io, k)
+        for k, v in zip("eh", og.field(cp, ob.blocks, *s, enei, io)):
+            ref = g["{}_field{}_{}".format(tag, io, k)]
+            assert rel(v.reshape(ref.shape), ref) < 1e-13, (io, k)
+    for i, j, key in ((0, 0, "H1p"), (1, 1, "H2p"), (1, 1, "Gp"), (0, 0, "Gp")):
+        M = og.green_region(cp, ob.blocks, i, j, key, enei)
+        nm = "{}_{}{}{}".format(tag, key, i, j)
+        assert rel(M[:8], g[nm + "_rows"]) < 1e-13, nm
+        assert abs(np.sum(np.abs(M)) - g[nm + "_abssum"]) <= 1e-12 * g[nm + "_abssum"], nm

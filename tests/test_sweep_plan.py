@@ -145,12 +145,3 @@ def test_autotune_picks_the_fastest_schedule():
                                  solver_factory=factory)
     assert set(rates) == {(1, "interleave"), (4, "interleave"), (16, "interleave")}
     assert best == (4, "interleave"), rates
-
-
-def test_bemret_potential_and_field_say_not_implemented():
-    import pytest
-    from mnpbem_b200.bem import BEMRet
-    with pytest.raises(NotImplementedError):
-        BEMRet.potential(None, None)
-    with pytest.raises(NotImplementedError):
-        BEMRet.field(None, None)
