@@ -197,12 +197,25 @@ int bem200_gemm(int dtype, int engine, int m, int n, int k, const double* alpha,
                 const void* B, int64_t ldb, const double* beta, void* C, int64_t ldc, void* ws, size_t ws_bytes,
                 void* stream);
 size_t bem200_gemm_workspace_size(int engine, int m, int n, int k);
-/* In-place P A = L U with partial pivoting (largest |re|+|im|).  Rows are
- * not moved: logical row i of P A (and of L, U) is storage row rowmap[i].
- * ipiv[k] = logical row exchanged with row k (LAPACK swap sequence, 0-based);
- * *info = first exactly-zero pivot (1-based) or 0.  All arrays are device. */
+/* In-place P A = L U.  Rows are not moved: logical row i of P A (and of L,
+ * U) is storage row rowmap[i].  ipiv[k] = logical row exchanged with row k
+ * (LAPACK swap sequence, 0-based); *info = first exactly-zero pivot (1-based)
+ * or 0.  All arrays are device.
+ * complex128: partial pivoting (largest |re|+|im|), LAPACK's pivots.
+ * complex64: panels of more than 512 rows choose their 32 pivot rows by
+ * tournament pivoting (each CTA of a cluster nominates the pivots of its own
+ * rows, one CTA factors the nominees; Grigori, Demmel & Xiang, SIAM J.
+ * Matrix Anal. Appl. 32, 2011): one cluster-wide exchange per panel instead
+ * of one per column, pivots that may differ from LAPACK's.  Shorter panels
+ * use partial pivoting.  Replaces the LU factorisations of BEMRet.init
+ * (mnpbem/bem/bem_ret.py:437-523, via mnpbem/utils/gpu.py:145).
+ * bem200_getrf_ex: flags BEM200_GETRF_PARTIAL_PIVOTING = partial pivoting
+ * for complex64 too. */
+#define BEM200_GETRF_PARTIAL_PIVOTING 1
 int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
                  int32_t* info, void* ws, size_t ws_bytes, void* stream);
+int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
+                    int32_t* info, void* ws, size_t ws_bytes, int flags, void* stream);
 /* ws of this size lets bem200_getrf run its look-ahead schedule: panels on a
  * high-priority stream, trailing updates on a low-priority one, both forked
  * from and joined back into `stream` (same pivots and factors).  A smaller

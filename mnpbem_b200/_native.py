@@ -60,6 +60,8 @@ _SIGS = {
     "bem200_gemm_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "bem200_getrf": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _i64, _vp, _vp, _vp, _vp, _sz,
                                     _vp]),
+    "bem200_getrf_ex": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _i64, _vp, _vp, _vp, _vp, _sz,
+                                       ctypes.c_int, _vp]),
     "bem200_getrf_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "bem200_getrs_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "bem200_getrs": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _i64, _vp, _vp,

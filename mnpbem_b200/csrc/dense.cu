@@ -893,9 +893,222 @@ __global__ void __launch_bounds__(kPushThreads, 1) panel_lu_grid_kernel(int m, i
   }
 }
 
+// ----------------------------------------------------------------------------
+// Tournament-pivoting panel (communication-avoiding LU, Grigori, Demmel & Xiang,
+// SIAM J. Matrix Anal. Appl. 32 (2011)) for the complex64 factors, whose
+// accuracy is restored by iterative refinement: the pivot rows of a panel are
+// chosen with one cluster-wide exchange per panel instead of one per column.
+//   1. every CTA of the cluster factors its own rows with partial pivoting
+//      (block barriers only) and nominates its (up to) 32 pivot rows;
+//   2. CTA 0 gathers the nominated rows' ORIGINAL values and factors them with
+//      partial pivoting: its pivot sequence is the panel's, and the pivot rows
+//      after elimination are [L11 \ U11];
+//   3. every CTA rewrites its rows: pivot rows get their [L11 \ U11] row, the
+//      others L21 = A21 U11^-1 from their original values.
+// One row per thread (registers); three cluster barriers per panel.
+constexpr int kCaluThreads = 512;
+constexpr int kCaluWarps = kCaluThreads / 32;
+constexpr int kCaluMaxCluster = 16;
+constexpr int kCaluMinRows = 512;  // shorter panels fit one CTA: exact partial pivoting (push panel)
+
+template <typename C>
+struct CaluShared {
+  C wrow[2][kCaluWarps][kPanelNB];  // each warp's best row, double buffered
+  R_t<C> wval[2][kCaluWarps];
+  int widx[2][kCaluWarps];
+  int lperm[kPanelNB];                          // this CTA's local pivot rows (panel row ids)
+  int cand[kCaluMaxCluster * kPanelNB];         // CTA 0: nominated rows of every CTA
+  int ncand[kCaluMaxCluster];                   // CTA 0: how many each CTA nominated
+  int perm[kPanelNB];                           // the panel's pivot rows
+  C lu11[kPanelNB][kPanelNB];                   // [L11 \ U11], row t = pivot row t after elimination
+  C uinv[kPanelNB];
+  int singular;
+  int nsteps;
+};
+
+// Partial-pivoting LU of the rows held by this CTA's threads (row `rid` in v,
+// `act` = thread holds a row), w columns.  Records the pivot row ids in
+// piv_out and, when lu_out is set, the pivot rows after elimination.  Returns
+// the number of pivot steps taken (fewer than w when the CTA runs out of
+// rows).  All threads of the CTA call it.
+template <typename C>
+__device__ __forceinline__ int calu_local(CaluShared<C>& sh, C (&v)[kPanelNB], bool act, int rid, int w, int* piv_out,
+                          C (*lu_out)[kPanelNB], int* singular) {
+  using Real = R_t<C>;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned kFull = 0xffffffffu;
+  int steps = w;
+#pragma unroll 1
+  for (int t = 0; t < w; ++t) {
+    const int buf = t & 1;
+    C vt = v[0];
+#pragma unroll
+    for (int c = 1; c < kPanelNB; ++c)
+      if (c == t) vt = v[c];
+    Real wb = act ? pmag(vt) : (Real)-1;
+    int wi = act ? rid : INT_MAX;
+    warp_argmax<C>(wb, wi);
+    if (act && wi == rid) {
+#pragma unroll
+      for (int c = 0; c < kPanelNB; ++c) sh.wrow[buf][wid][c] = v[c];
+    }
+    if (lane == 0) {
+      sh.wval[buf][wid] = wb;
+      sh.widx[buf][wid] = wi;
+    }
+    __syncthreads();
+    Real b = lane < kCaluWarps ? sh.wval[buf][lane] : (Real)-1;
+    int bi = lane < kCaluWarps ? sh.widx[buf][lane] : INT_MAX;
+    const Real b0 = b;
+    const int i0 = bi;
+    warp_argmax<C>(b, bi);
+    if (bi == INT_MAX) {  // no row left in this CTA (uniform)
+      steps = t;
+      break;
+    }
+    const unsigned msk = __ballot_sync(kFull, lane < kCaluWarps && i0 == bi && b0 == b);
+    const int ww = msk ? __ffs(msk) - 1 : 0;
+    const C* prow = sh.wrow[buf][ww];
+    if (threadIdx.x == 0) {
+      piv_out[t] = bi;
+      if (singular && !(b > 0) && !*singular) *singular = t + 1;
+    }
+    if (lu_out && wid == 0) lu_out[t][lane] = prow[lane];
+    const C piv = prow[t];
+    const C inv = cabs1(piv) > 0 ? cdiv(cmake<C>(1.0, 0.0), piv) : czero<C>();
+    if (rid == bi) act = false;
+    if (act) {
+      const C l = cmul(vt, inv);
+#pragma unroll
+      for (int g = 0; g < kPanelNB; g += 8) {
+        if (g + 7 >= t) {
+#pragma unroll
+          for (int c = g; c < g + 8; ++c) {
+            const C u = csub(v[c], cmul(l, prow[c]));
+            v[c] = (c > t) ? u : ((c == t) ? l : v[c]);
+          }
+        }
+      }
+    }
+  }
+  return steps;
+}
+
+template <typename C>
+__global__ void __launch_bounds__(kCaluThreads, 1) panel_calu_kernel(int m, int w, C* __restrict__ A, long long ld,
+                                                                    int col, int32_t* __restrict__ rowmap,
+                                                                    int32_t* __restrict__ ipiv, int ipiv_base,
+                                                                    int* __restrict__ info, int R) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int cs = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  __shared__ CaluShared<C> sh;
+  const int tid = threadIdx.x;
+  const int r0 = rank * R;
+  const int rcount = max(0, min(R, m - r0));
+  const int rid = r0 + tid;  // panel row of this thread
+  const bool mine = tid < rcount;
+  const long long phys = mine ? (long long)rowmap[rid] : 0;
+  C v[kPanelNB];
+#pragma unroll
+  for (int c = 0; c < kPanelNB; ++c) v[c] = (mine && c < w) ? A[phys * ld + col + c] : czero<C>();
+  if (tid == 0) sh.singular = 0;
+  __syncthreads();
+  // 1. local partial pivoting; nominate the pivot rows to CTA 0
+  const int nloc = calu_local<C>(sh, v, mine, rid, w, sh.lperm, nullptr, nullptr);
+  __syncthreads();  // thread 0 wrote the last pivot after the last barrier of the sweep
+  {
+    CaluShared<C>* dst = cluster.map_shared_rank(&sh, 0);
+    if (tid < nloc) dst->cand[rank * kPanelNB + tid] = sh.lperm[tid];
+    if (tid == 0) dst->ncand[rank] = nloc;
+  }
+  cluster.sync();
+  // 2. CTA 0: the tournament over the nominated rows' original values
+  if (rank == 0) {
+    int k = tid, src = -1;
+    for (int r = 0; r < cs && src < 0; ++r) {
+      if (k < sh.ncand[r]) src = sh.cand[r * kPanelNB + k];
+      else k -= sh.ncand[r];
+    }
+    const bool have = src >= 0;
+    const long long sp = have ? (long long)rowmap[src] : 0;
+#pragma unroll
+    for (int c = 0; c < kPanelNB; ++c) v[c] = (have && c < w) ? A[sp * ld + col + c] : czero<C>();
+    const int steps = calu_local<C>(sh, v, have, have ? src : INT_MAX - 1 - tid, w, sh.perm, sh.lu11, &sh.singular);
+    if (tid == 0) sh.nsteps = steps;
+  }
+  cluster.sync();
+  // 3. every CTA: pivot rows take [L11 \ U11], the others L21 = A21 U11^-1
+  if (rank != 0) {
+    const CaluShared<C>* src = cluster.map_shared_rank(&sh, 0);
+    for (int idx = tid; idx < kPanelNB * kPanelNB; idx += kCaluThreads) {
+      const int r = idx / kPanelNB, c = idx % kPanelNB;
+      sh.lu11[r][c] = src->lu11[r][c];
+    }
+    if (tid < kPanelNB) sh.perm[tid] = src->perm[tid];
+    if (tid == 0) sh.nsteps = src->nsteps;
+  }
+  cluster.sync();  // CTA 0's shared memory is no longer read remotely after this point
+  if (tid < kPanelNB) {
+    const C d = sh.lu11[tid][tid];
+    sh.uinv[tid] = (tid < w && cabs1(d) > 0) ? cdiv(cmake<C>(1.0, 0.0), d) : czero<C>();
+  }
+  __syncthreads();
+  if (mine) {
+    int t_own = -1;
+    for (int t = 0; t < w; ++t)
+      if (sh.perm[t] == rid) t_own = t;
+    if (t_own >= 0) {
+      for (int c = 0; c < w; ++c) A[phys * ld + col + c] = sh.lu11[t_own][c];
+    } else {
+      // x U11 = a for the original row a: x_k = a_k / U_kk, then a_c -= x_k U_kc
+      // (c > k); columns >= w hold zeros and stay zero
+#pragma unroll
+      for (int c = 0; c < kPanelNB; ++c) v[c] = (c < w) ? A[phys * ld + col + c] : czero<C>();
+#pragma unroll
+      for (int k = 0; k < kPanelNB; ++k) {
+        v[k] = cmul(v[k], sh.uinv[k]);
+#pragma unroll
+        for (int c = k + 1; c < kPanelNB; ++c) v[c] = csub(v[c], cmul(v[k], sh.lu11[k][c]));
+      }
+#pragma unroll
+      for (int c = 0; c < kPanelNB; ++c)
+        if (c < w) A[phys * ld + col + c] = v[c];
+    }
+  }
+  if (rank == 0 && (tid >> 5) == 0) {
+    replay_pivots(w, sh.perm, ipiv, ipiv_base, rowmap);
+    if ((tid & 31) == 0 && sh.singular && info) atomicCAS(info, 0, ipiv_base + sh.singular);
+  }
+}
+
 template <typename C>
 static int panel_lu(const LaContext& ctx, int m, int w, C* A, long long ld, int col, int32_t* rowmap, int32_t* ipiv,
                     int ipiv_base) {
+  if constexpr (sizeof(C) == 8) {
+    if (ctx.tournament && m > kCaluMinRows && m <= kCaluMaxCluster * kCaluThreads) {
+      // complex64: tournament pivoting, 128 - 512 rows per CTA
+      const int cs = min(kCaluMaxCluster, ceil_div(m, 128));
+      const int R = ceil_div(m, cs);
+      auto kern = panel_calu_kernel<C>;
+      BEM_CUDA_CHECK(set_kernel_attrs_once(kern, 0, true));
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(cs, 1, 1);
+      cfg.blockDim = dim3(kCaluThreads, 1, 1);
+      cfg.dynamicSmemBytes = 0;
+      cfg.stream = ctx.stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = cs;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      BEM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, m, w, A, ld, col, rowmap, ipiv, ipiv_base, ctx.dinfo, R));
+      count_launch();
+      return BEM200_OK;
+    }
+  }
   if (m <= kPushMaxCluster * kPushThreads) {
     // 128 - 384 rows per CTA, as many CTAs (<= 16) as that takes
     const int cs = min(kPushMaxCluster, max(1, ceil_div(m, 128)));
@@ -1699,14 +1912,16 @@ size_t bem200_getrf_workspace_size(int dtype, int engine, int n) {
   return ((gemm_tc_workspace(n, n, n, engine_of(engine)) + 255) & ~size_t(255)) + getrf_snap_bytes(n);
 }
 
-int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv, int32_t* info,
-                 void* ws, size_t ws_bytes, void* stream) {
+int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv, int32_t* info,
+                    void* ws, size_t ws_bytes, int flags, void* stream) {
+  BEM_REQUIRE((flags & ~BEM200_GETRF_PARTIAL_PIVOTING) == 0, BEM200_ERR_ARG, "getrf: unknown flags 0x%x", flags);
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
   ctx.engine = engine_of(engine);
   ctx.ws = ws;
   ctx.ws_bytes = ws_bytes;
   ctx.dinfo = info;
+  ctx.tournament = (flags & BEM200_GETRF_PARTIAL_PIVOTING) == 0;
   int32_t* snap = nullptr;
   if (ws && n > 0 && ws_bytes >= bem200_getrf_workspace_size(dtype, engine, n)) {
     const size_t sb = getrf_snap_bytes(n);
@@ -1717,6 +1932,11 @@ int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* row
   if (dtype == BEM200_C64) return getrf<float2>(ctx, n, (float2*)A, ld, rowmap, ipiv, snap);
   set_error("getrf: bad dtype %d", dtype);
   return BEM200_ERR_ARG;
+}
+
+int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv, int32_t* info,
+                 void* ws, size_t ws_bytes, void* stream) {
+  return bem200_getrf_ex(dtype, engine, n, A, ld, rowmap, ipiv, info, ws, ws_bytes, 0, stream);
 }
 
 size_t bem200_getrs_workspace_size(int dtype, int n, int nrhs) {

@@ -3,7 +3,7 @@
     python -m mnpbem_b200.microbench step  [--faces 1444] [--precision mixed|fp64] [--steps 1] [--warmup 1]
     python -m mnpbem_b200.microbench green [--faces 1444] [--dtype c128|c64] [--reps 3]
     python -m mnpbem_b200.microbench gemm  [--m 5768 --n 2884 --k 2884] [--engine 1] [--reps 3]
-    python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1]
+    python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1] [--partial]
     python -m mnpbem_b200.microbench hmat  [--faces 1444] [--cleaf 200] [--htol 1e-6] [--reps 3]
     python -m mnpbem_b200.microbench iter  [--faces 1444] [--hmatrix] [--noprecond] [--tol 1e-10]
     python -m mnpbem_b200.microbench large [--side 3 | --shape cube] [--hmatrix] [--tol 1e-8]
@@ -123,11 +123,22 @@ def case_getrf(a):
     wsb = int(nat.lib().bem200_getrf_workspace_size(code, a.engine, n))
     ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
 
+    flags = 1 if a.partial else 0
+
     def go():
         A.copy_(A0)
-        nat.call("bem200_getrf", code, a.engine, n, nat.ptr(A), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info),
-                 nat.ptr(ws), wsb, nat.stream_ptr())
+        nat.call("bem200_getrf_ex", code, a.engine, n, nat.ptr(A), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info),
+                 nat.ptr(ws), wsb, flags, nat.stream_ptr())
     go()
+    # backward error of a solve with these factors: |A0 x - b| / (|A0| |x|)
+    b = torch.randn(n, 2, dtype=dt, device="cuda", generator=gen)
+    x = b.clone()
+    scr = torch.empty(int(nat.lib().bem200_getrs_workspace_size(code, n, 2)), dtype=torch.uint8, device="cuda")
+    nat.call("bem200_getrs", code, 0, n, 2, nat.ptr(A), n, nat.ptr(rowmap), nat.ptr(x), 2, None, 0, nat.ptr(scr),
+             None, nat.stream_ptr())
+    A64, x64 = A0.to(torch.complex128), x.to(torch.complex128)
+    berr = float(torch.linalg.matrix_norm(A64 @ x64 - b.to(torch.complex128), ord=float("inf"))
+                 / (torch.linalg.matrix_norm(A64, ord=float("inf")) * torch.linalg.matrix_norm(x64, ord=float("inf"))))
     if a.graph:
         # the same factorisation replayed from a CUDA graph (no host launch work)
         torch.cuda.synchronize()
@@ -138,8 +149,9 @@ def case_getrf(a):
         ms = _timed(g.replay, a.reps)
     else:
         ms = _timed(go, a.reps)
-    return {"case": "getrf", "n": n, "dtype": a.dtype, "engine": a.engine, "graph": bool(a.graph), "ms": ms,
-            "TFLOPs": 8.0 / 3.0 * n ** 3 / ms / 1e9, "info": int(info.item())}
+    return {"case": "getrf", "n": n, "dtype": a.dtype, "engine": a.engine, "graph": bool(a.graph),
+            "pivoting": "partial" if a.partial else "tournament (complex64 panels > 512 rows)", "ms": ms,
+            "TFLOPs": 8.0 / 3.0 * n ** 3 / ms / 1e9, "info": int(info.item()), "backward_error": berr}
 
 
 def case_hmat(a):
@@ -386,6 +398,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--graph", action="store_true", help="getrf: replay from a CUDA graph")
+    ap.add_argument("--partial", action="store_true", help="getrf: partial pivoting for complex64 too")
     ap.add_argument("--cleaf", type=int, default=200)
     ap.add_argument("--htol", type=float, default=1e-6)
     ap.add_argument("--tol", type=float, default=1e-10)

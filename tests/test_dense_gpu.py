@@ -186,3 +186,45 @@ def test_getrf_lookahead_tall_panel_c128(cuda):
     np.testing.assert_array_equal(ipiv.cpu().numpy(), piv)
     got = At.cpu().numpy()[rowmap.cpu().numpy()]
     assert np.max(np.abs(got - lu)) / np.max(np.abs(lu)) < 1e-10
+
+
+@pytest.mark.parametrize("n", [700, 3000, 5768])
+def test_getrf_c64_tournament_pivoting(cuda, n):
+    """complex64 panels of more than 512 rows pick their pivots by tournament
+    (one cluster exchange per panel).  The factors solve as accurately as the
+    partial-pivoting ones (BEM200_GETRF_PARTIAL_PIVOTING): backward error of a
+    solve within a small factor of it and at the complex64 rounding level."""
+    import torch
+    A = _rand(n, n, 900 + n).astype(np.complex64)
+    B = _rand(n, 2, 901 + n).astype(np.complex64)
+    A64 = A.astype(np.complex128)
+    berr = []
+    for flags in (0, 1):
+        At = _t(A)
+        rowmap = torch.empty(n, dtype=torch.int32, device="cuda")
+        ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
+        info = torch.zeros(1, dtype=torch.int32, device="cuda")
+        wsb = int(nat.lib().bem200_getrf_workspace_size(nat.C64, 1, n))
+        ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+        nat.call("bem200_getrf_ex", nat.C64, 1, n, nat.ptr(At), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info),
+                 nat.ptr(ws), wsb, flags, nat.stream_ptr())
+        assert int(info.item()) == 0
+        perm = rowmap.cpu().numpy()
+        assert sorted(perm.tolist()) == list(range(n))      # a permutation
+        Bt = _t(B)
+        getrs(At, rowmap, Bt)
+        X = Bt.cpu().numpy().astype(np.complex128)
+        r = A64 @ X - B
+        berr.append(np.max(np.abs(r)) / (np.max(np.sum(np.abs(A64), axis=1)) * np.max(np.abs(X))))
+    assert berr[0] < 1e-5 and berr[0] < 10 * berr[1] + 1e-7, berr
+
+
+def test_getrf_c64_tournament_zero_column(cuda):
+    """A zero column inside a tall complex64 panel is reported as a zero pivot."""
+    import torch
+    n = 1200
+    A = (_rand(n, n, 41) + 3 * np.eye(n)).astype(np.complex64)
+    A[:, 10] = 0
+    At = _t(A)
+    rowmap, ipiv, info = _getrf_ws(At, 1)
+    assert int(info.item()) == 11
