@@ -319,6 +319,61 @@ int bem200_bem_precond(int precision, int engine, int n, int npol, void* ws, con
                        const double* eps1, const double* eps2, const double* nvec, double k0, void* y,
                        void* scratch, void* gemm_ws, size_t gemm_ws_bytes, void* stream);
 
+/* Transposed solve and operator, for reverse-mode derivatives (one transposed
+ * solve gives the gradient of a functional of the solution over every
+ * parameter; the reference has no gradients, so these have no counterpart
+ * call -- they transpose BEMRet.solve, mnpbem/bem/bem_ret.py:1569-1831, and
+ * BEMRetIter._afun, mnpbem/bem/bem_ret_iter.py:1362-1501).  Pairings are
+ * bilinear (no conjugation).
+ * bem200_bem_solve_T: b = S^T cot with S = the factored solve of
+ *   bem200_bem_solve (Eqs. 19-20): cot in the solution layout [W1 | W2]
+ *   (8 n p complex128), b in the right-hand-side layout.  Every step of the
+ *   solve transposed: transposed LU solves with the factors' row maps,
+ *   transposed products with Delta^-1 and Sigma1.  precision 1 applies the
+ *   complex64 factors once (to cot scaled to unit max-norm), the transposed
+ *   counterpart of bem200_bem_precond; npol <= 4.
+ * bem200_bem_apply_T: r = A^T l (w NULL) or r = w - A^T l for the FP64 BEM
+ *   operator of bem200_bem_apply; l in the right-hand-side layout, w and r in
+ *   the solution layout.  Refining S^T with it gives A^-T to FP64 accuracy. */
+size_t bem200_bem_solve_T_workspace_size(int precision, int n, int npol);
+int bem200_bem_solve_T(int precision, int engine, int n, int npol, void* ws, const void* cot, int eps_per_face,
+                       const double* eps1, const double* eps2, const double* nvec, double k0, void* b, void* scratch,
+                       void* stream);
+size_t bem200_bem_apply_T_workspace_size(int n, int npol);
+int bem200_bem_apply_T(int n, int npol, const void* G1, const void* G2, const void* H1, const void* H2,
+                       int eps_per_face, const double* eps1, const double* eps2, const double* nvec, double k0,
+                       const void* l, const void* w, void* r, void* scratch, void* stream);
+
+/* bem200_shape_gradient: c = lambda^T (dA/dtheta) x contracted over every face
+ * pair at once, for the geometry parameters theta of all faces: grad
+ * (complex128, 40 n) = pos (n, 3) | nvec (n, 3) | area (n) | tvec1 (n, 3) |
+ * tvec2 (n, 3) | face nodes (n, 9, 3).  x = (W1, W2) is the solution, lam
+ * the adjoint (right-hand-side layout, e.g. from bem200_bem_solve_T), npol <=
+ * 4.  Far pairs are differentiated analytically and swept by rows and by
+ * columns without storing any n x n matrix; refined pairs through their
+ * phase, normals and coefficients, whose derivatives with respect to the
+ * face nodes and the observation frame are exact (forward-mode dual numbers
+ * over the refinement quadrature); the closed-surface correction is chained
+ * through its column sums.  Inputs: the assembly tables of
+ * bem200_green_assemble (pid, blk_mat, kmat_host), the refinement inputs of
+ * bem200_refine_integrals (nodes, face_kind, rules), the refinement tables in
+ * CSR form (ref_row_ptr) and by column (csc_col_ptr (n + 1), csc_row), the
+ * coefficients g and f after the closed-surface correction, corr (n) and
+ * closed_mask of bem200_closed_correction.  No counterpart in the reference
+ * (which has no gradients); it differentiates the assembly of
+ * mnpbem/greenfun/greenret_refined.py:654-867 and compgreen_ret.py:192-400
+ * within the operator of mnpbem/bem/bem_ret_iter.py:1362-1501. */
+size_t bem200_shape_gradient_workspace_size(int n, int64_t nref, int order);
+int bem200_shape_gradient(int n, int npol, int npart, const int32_t* pid, const int32_t* blk_mat, int nmat,
+                          const double* kmat_host, double k0, int eps_per_face, const double* eps1,
+                          const double* eps2, const uint64_t* closed_mask, const double* pos, const double* nvec,
+                          const double* tvec1, const double* tvec2, const double* area, const double* nodes,
+                          const int32_t* face_kind, const double* rules, int n28, int n3, int n4, int64_t nref,
+                          const int64_t* ref_row_ptr, const int32_t* ref_row, const int32_t* ref_col,
+                          const int8_t* ref_kind, const int64_t* csc_col_ptr, const int32_t* csc_row, int order,
+                          const double* g, const double* f, const double* corr, const void* W1, const void* W2,
+                          const void* lam, void* grad, void* scratch, void* stream);
+
 /* x = the right-hand side b relabelled into the solution layout (phi -> sig1,
  * a -> h1, De -> sig2, alpha -> h2): the M = I "preconditioner" of the
  * unpreconditioned iteration, which pairs the two spaces as the reference's

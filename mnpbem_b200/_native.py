@@ -82,6 +82,17 @@ _SIGS = {
     "bem200_bem_solve_ir": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
                                            ctypes.c_int, _vp, _vp, _vp, _dbl, _dbl, ctypes.c_int, _vp, _vp, _vp, _vp,
                                            _sz, _vp, _vp, _vp]),
+    "bem200_bem_solve_T_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "bem200_bem_solve_T": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                          ctypes.c_int, _vp, _vp, _vp, _dbl, _vp, _vp, _vp]),
+    "bem200_bem_apply_T_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int]),
+    "bem200_bem_apply_T": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp,
+                                          _vp, _dbl, _vp, _vp, _vp, _vp, _vp]),
+    "bem200_shape_gradient_workspace_size": (_sz, [ctypes.c_int, _i64, ctypes.c_int]),
+    "bem200_shape_gradient": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp,
+                                             _dbl, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64, _vp, _vp, _vp, _vp, _vp,
+                                             _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bem200_convert_c128_c64": (ctypes.c_int, [_i64, _vp, _vp, _vp]),
     "bem200_bem_precond": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                           ctypes.c_int, _vp, _vp, _vp, _dbl, _vp, _vp, _vp, _sz, _vp]),

@@ -18,7 +18,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libbem200.so")
 
 SOURCES = ["green.cu", "dense.cu", "gemm_tc.cu", "bem.cu", "krylov.cu", "hmat.cu", "planewave.cu", "field.cu",
-           "noalloc.cu"]
+           "adjoint.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                      "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]

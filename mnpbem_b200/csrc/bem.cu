@@ -342,6 +342,280 @@ static int bem_solve_core(const LaContext& ctx0, int n, int p, void* ws, const C
   return BEM200_OK;
 }
 
+// ------------------------------------------------------------ transposed solve
+// S^T of the solve above (S = A^-1 as computed by bem_solve_core), for the
+// reverse-mode derivatives: unknown-space cotangents (W1c = [s1 | h1], W2c =
+// [s2 | h2], n x 4p) -> equation-space cotangents (phi, a, alpha, De, the
+// right-hand-side layout).  Every step of bem_solve_core transposed, in reverse
+// order: G^-T and Sigma^-T are transposed LU solves, (Delta^-1)^T and Sigma1^T
+// transposed products, the eps and normal products their own transposes.
+
+// Bs = us1 + u2s, Bh = uh1 + u2h; phi_o = us1, a_o = uh1
+template <typename C>
+__global__ void tsolve_start_kernel(int n, int p, const C* __restrict__ U1, const C* __restrict__ U2, C* __restrict__ Bs,
+                                    C* __restrict__ Bh, C* __restrict__ phi_o, C* __restrict__ a_o) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * 4 * p) return;
+  const int i = (int)(idx / (4 * p)), c = (int)(idx % (4 * p));
+  const C s = cadd(U1[idx], U2[idx]);
+  if (c < p) {
+    Bs[(long long)i * p + c] = s;
+    phi_o[(long long)i * p + c] = U1[idx];
+  } else {
+    Bh[(long long)i * 3 * p + (c - p)] = s;
+    a_o[(long long)i * 3 * p + (c - p)] = U1[idx];
+  }
+}
+
+// Bs += ik L (n . w)
+template <typename C>
+__global__ void tsolve_addnw_kernel(int n, int p, const C* __restrict__ w, const double* __restrict__ nvec, EpsArg eps,
+                                    double k0, C* __restrict__ Bs) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * p) return;
+  const int i = (int)(idx / p), q = (int)(idx % p);
+  const double2 L = csub(eps_at(eps, i, false), eps_at(eps, i, true));
+  double2 dot = make_double2(0, 0);
+  for (int c = 0; c < 3; ++c) {
+    const C x = w[((long long)i * 3 + c) * p + q];
+    dot = cadd(dot, cscale(make_double2(x.x, x.y), nvec[3 * i + c]));
+  }
+  const C b = Bs[idx];
+  Bs[idx] = to_c<C>(cadd(make_double2(b.x, b.y), cmul(make_double2(0.0, k0), cmul(L, dot))));
+}
+
+// T = L n (x) (ik v)   (n x 3p)
+template <typename C>
+__global__ void tsolve_lift_kernel(int n, int p, const C* __restrict__ v, const double* __restrict__ nvec, EpsArg eps,
+                                   double k0, C* __restrict__ T) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * 3 * p) return;
+  const int i = (int)(idx / (3 * p)), c = (int)((idx / p) % 3), q = (int)(idx % p);
+  const double2 L = csub(eps_at(eps, i, false), eps_at(eps, i, true));
+  const C x = v[(long long)i * p + q];
+  T[idx] = to_c<C>(cscale(cmul(make_double2(0.0, k0), cmul(L, make_double2(x.x, x.y))), nvec[3 * i + c]));
+}
+
+// VA = [v | w + t2]  (n x 4p);  De_o = v
+template <typename C>
+__global__ void tsolve_va_kernel(int n, int p, const C* __restrict__ v, const C* __restrict__ w,
+                                 const C* __restrict__ t2, C* __restrict__ VA, C* __restrict__ De_o) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * 4 * p) return;
+  const int i = (int)(idx / (4 * p)), c = (int)(idx % (4 * p));
+  if (c < p) {
+    const C x = v[(long long)i * p + c];
+    VA[idx] = x;
+    De_o[(long long)i * p + c] = x;
+  } else {
+    const long long o = (long long)i * 3 * p + (c - p);
+    VA[idx] = cadd(w[o], t2[o]);
+  }
+}
+
+// phi_o += -L1 SDT + ik L1 (n . alpham);  a_o += ik L1 (n (x) v) - SAT;  alpha_o = alpham
+// with VA = [v | alpham] and SD = Sigma1^T VA = [SDT | SAT]
+template <typename C>
+__global__ void tsolve_finish_kernel(int n, int p, const C* __restrict__ VA, const C* __restrict__ SD,
+                                     const double* __restrict__ nvec, EpsArg eps, double k0, C* __restrict__ phi_o,
+                                     C* __restrict__ a_o, C* __restrict__ alpha_o) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * p) return;
+  const int i = (int)(idx / p), q = (int)(idx % p);
+  const double2 e1 = eps_at(eps, i, false);
+  const double2 ik = make_double2(0.0, k0);
+  const C* va = VA + (long long)i * 4 * p;
+  const C* sd = SD + (long long)i * 4 * p;
+  const double nv[3] = {nvec[3 * i], nvec[3 * i + 1], nvec[3 * i + 2]};
+  double2 nal = make_double2(0, 0);
+  const C vq = va[q];
+  const double2 ikL1v = cmul(ik, cmul(e1, make_double2(vq.x, vq.y)));
+  for (int c = 0; c < 3; ++c) {
+    const C al = va[p + c * p + q];
+    nal = cadd(nal, cscale(make_double2(al.x, al.y), nv[c]));
+    const long long ai = ((long long)i * 3 + c) * p + q;
+    const C sa = sd[p + c * p + q];
+    const C ao = a_o[ai];
+    a_o[ai] = to_c<C>(csub(cadd(make_double2(ao.x, ao.y), cscale(ikL1v, nv[c])), make_double2(sa.x, sa.y)));
+    alpha_o[ai] = al;
+  }
+  const C sdt = sd[q];
+  const C po = phi_o[idx];
+  double2 ph = make_double2(po.x, po.y);
+  ph = csub(ph, cmul(e1, make_double2(sdt.x, sdt.y)));
+  ph = cadd(ph, cmul(ik, cmul(e1, nal)));
+  phi_o[idx] = to_c<C>(ph);
+}
+
+template <typename C>
+static size_t solve_T_scratch_bytes(int n, int p) {
+  return align256(sizeof(C) * (size_t)n * p * 29) + align256(solve_left_scratch_bytes<C>(n, 4 * p)) +
+         align256(gemm_t_scratch_bytes<C>(n, 4 * p));
+}
+
+// cot = [W1c | W2c] (8np, solution layout) -> b (8np, right-hand-side layout)
+template <typename C>
+static int bem_solve_T_core(const LaContext& ctx0, int n, int p, void* ws, const C* cot, const EpsArg& eps,
+                            const double* nvec, double k0, C* b, void* scratch) {
+  BemState<C> s = state_view<C>(n, ws);
+  LaContext ctx = ctx0;
+  ctx.dstatus = s.status;
+  cudaStream_t st_ = ctx.stream;
+  const long long np = (long long)n * p;
+  char* base = reinterpret_cast<char*>(scratch);
+  C* U1 = reinterpret_cast<C*>(base);  // n x 4p
+  C* U2 = U1 + 4 * np;                 // n x 4p
+  C* Bs = U2 + 4 * np;                 // n x p
+  C* Bh = Bs + np;                     // n x 3p
+  C* w = Bh + 3 * np;                  // n x 3p
+  C* T = w + 3 * np;                   // n x 3p
+  C* t2 = T + 3 * np;                  // n x 3p
+  C* VA = t2 + 3 * np;                 // n x 4p
+  C* SD = VA + 4 * np;                 // n x 4p   (29 np)
+  void* lscr = base + align256(sizeof(C) * (size_t)np * 29);
+  void* tscr = reinterpret_cast<char*>(lscr) + align256(solve_left_scratch_bytes<C>(n, 4 * p));
+  C* phi_o = b;
+  C* a_o = b + np;
+  C* alpha_o = b + 4 * np;
+  C* De_o = b + 7 * np;
+  const C one = cmake<C>(1.0, 0.0), zero = czero<C>();
+  int st;
+  BEM_CUDA_CHECK(cudaMemcpyAsync(U1, cot, sizeof(C) * 8 * np, cudaMemcpyDeviceToDevice, st_));
+  if ((st = solve_left_T<C>(ctx, n, 4 * p, s.M[0], n, s.map[0], U1, 4 * p, lscr))) return st;
+  if ((st = solve_left_T<C>(ctx, n, 4 * p, s.M[1], n, s.map[1], U2, 4 * p, lscr))) return st;
+  tsolve_start_kernel<C><<<ceil_div(4 * np, 256), 256, 0, st_>>>(n, p, U1, U2, Bs, Bh, phi_o, a_o);
+  BEM_LAUNCH_CHECK();
+  // w = Delta^-T Bh
+  if ((st = gemm_t<C>(ctx, n, 3 * p, n, one, plain(s.M[5], n), plain(Bh, 3 * p), zero, plain(w, 3 * p), tscr)))
+    return st;
+  tsolve_addnw_kernel<C><<<ceil_div(np, 256), 256, 0, st_>>>(n, p, w, nvec, eps, k0, Bs);
+  BEM_LAUNCH_CHECK();
+  // v = Sigma^-T Bs (in place)
+  if ((st = solve_left_T<C>(ctx, n, p, s.M[6], n, s.map[3], Bs, p, lscr))) return st;
+  tsolve_lift_kernel<C><<<ceil_div(3 * np, 256), 256, 0, st_>>>(n, p, Bs, nvec, eps, k0, T);
+  BEM_LAUNCH_CHECK();
+  if ((st = gemm_t<C>(ctx, n, 3 * p, n, one, plain(s.M[5], n), plain(T, 3 * p), zero, plain(t2, 3 * p), tscr)))
+    return st;
+  tsolve_va_kernel<C><<<ceil_div(4 * np, 256), 256, 0, st_>>>(n, p, Bs, w, t2, VA, De_o);
+  BEM_LAUNCH_CHECK();
+  // Sigma1^T [v | alpham]
+  if ((st = gemm_t<C>(ctx, n, 4 * p, n, one, plain(s.M[2], n), plain(VA, 4 * p), zero, plain(SD, 4 * p), tscr)))
+    return st;
+  tsolve_finish_kernel<C><<<ceil_div(np, 256), 256, 0, st_>>>(n, p, VA, SD, nvec, eps, k0, phi_o, a_o, alpha_o);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+// ------------------------------------------------------------ transposed FP64 operator
+// A^T of the operator below, for equation-space cotangents l = (lphi, la,
+// lalpha, lDe) -> unknown-space (s1, h1 | s2, h2), solution layout:
+//   s1 =  G1^T lphi - ik e1 G1^T (n.lalpha) + e1 H1^T lDe
+//   s2 = -G2^T lphi + ik e2 G2^T (n.lalpha) - e2 H2^T lDe
+//   h1 =  G1^T la + H1^T lalpha - ik e1 G1^T (n lDe)
+//   h2 = -G2^T la - H2^T lalpha + ik e2 G2^T (n lDe)
+// U = [lphi | n.lalpha | la | n lDe] (n x 8p), V = [lDe | lalpha] (n x 4p).
+__global__ void opT_prep_kernel(int n, int p, const double2* __restrict__ l, const double* __restrict__ nvec,
+                                double2* __restrict__ U, double2* __restrict__ V) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long np = (long long)n * p;
+  if (idx >= np) return;
+  const int i = (int)(idx / p), q = (int)(idx % p);
+  const double2* lphi = l;
+  const double2* la = l + np;
+  const double2* lal = l + 4 * np;
+  const double2* lDe = l + 7 * np;
+  double2* u = U + (long long)i * 8 * p;
+  double2* v = V + (long long)i * 4 * p;
+  const double nv[3] = {nvec[3 * i], nvec[3 * i + 1], nvec[3 * i + 2]};
+  double2 na = make_double2(0, 0);
+  const double2 de = lDe[idx];
+  for (int c = 0; c < 3; ++c) {
+    const long long ai = ((long long)i * 3 + c) * p + q;
+    na = cadd(na, cscale(lal[ai], nv[c]));
+    u[2 * p + c * p + q] = la[ai];
+    u[5 * p + c * p + q] = cscale(de, nv[c]);
+    v[p + c * p + q] = lal[ai];
+  }
+  u[q] = lphi[idx];
+  u[p + q] = na;
+  v[q] = de;
+}
+
+__global__ void opT_combine_kernel(int n, int p, const double2* __restrict__ GU1, const double2* __restrict__ GU2,
+                                   const double2* __restrict__ HV1, const double2* __restrict__ HV2, EpsArg eps,
+                                   double k0, const double2* __restrict__ wv, double2* __restrict__ r) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long np = (long long)n * p;
+  if (idx >= 4 * np) return;
+  const int i = (int)(idx / (4 * p)), c = (int)(idx % (4 * p));
+  const double2 e1 = eps_at(eps, i, false), e2 = eps_at(eps, i, true);
+  const double2 ik = make_double2(0.0, k0);
+  const double2* g1 = GU1 + (long long)i * 8 * p;
+  const double2* g2 = GU2 + (long long)i * 8 * p;
+  const double2* h1 = HV1 + (long long)i * 4 * p;
+  const double2* h2 = HV2 + (long long)i * 4 * p;
+  double2 o1, o2;
+  if (c < p) {  // s
+    o1 = cadd(csub(g1[c], cmul(ik, cmul(e1, g1[p + c]))), cmul(e1, h1[c]));
+    o2 = csub(cadd(cscale(g2[c], -1.0), cmul(ik, cmul(e2, g2[p + c]))), cmul(e2, h2[c]));
+  } else {      // h, component (c - p)
+    const int hc = c - p;
+    o1 = csub(cadd(g1[2 * p + hc], h1[p + hc]), cmul(ik, cmul(e1, g1[5 * p + hc])));
+    o2 = cadd(csub(cscale(g2[2 * p + hc], -1.0), h2[p + hc]), cmul(ik, cmul(e2, g2[5 * p + hc])));
+  }
+  if (wv) {
+    o1 = csub(wv[idx], o1);
+    o2 = csub(wv[4 * np + idx], o2);
+  }
+  r[idx] = o1;
+  r[4 * np + idx] = o2;
+}
+
+static size_t apply_T_scratch_bytes(int n, int p) {
+  return align256(sizeof(double2) * (size_t)n * p * 32) + align256(gemm_t_scratch_bytes<double2>(n, 16));
+}
+
+static int bem_apply_T(const LaContext& ctx, int n, int p, const double2* G1, const double2* G2, const double2* H1,
+                       const double2* H2, const EpsArg& eps, const double* nvec, double k0, const double2* l,
+                       const double2* wv, double2* r, void* scratch) {
+  const long long np = (long long)n * p;
+  double2* U = reinterpret_cast<double2*>(scratch);  // n x 8p
+  double2* V = U + 8 * np;                           // n x 4p
+  double2* GU1 = V + 4 * np;                         // n x 8p
+  double2* GU2 = GU1 + 8 * np;                       // n x 8p
+  double2* HV1 = GU2 + 8 * np;                       // n x 4p
+  double2* HV2 = HV1 + 4 * np;                       // n x 4p   (32 np)
+  void* tscr = reinterpret_cast<char*>(scratch) + align256(sizeof(double2) * (size_t)np * 32);
+  opT_prep_kernel<<<ceil_div(np, 256), 256, 0, ctx.stream>>>(n, p, l, nvec, U, V);
+  BEM_LAUNCH_CHECK();
+  const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
+  int st;
+  // column blocks of at most 16 (8p columns for the G products, 4p for the H products)
+  for (int c0 = 0; c0 < 8 * p; c0 += 16) {
+    const int wc = min(16, 8 * p - c0);
+    RowView<double2> Ub{U, 8 * p, nullptr, c0};
+    if ((st = gemm_t<double2>(ctx, n, wc, n, one, plain(const_cast<double2*>(G1), n), Ub, zero,
+                              RowView<double2>{GU1, 8 * p, nullptr, c0}, tscr)))
+      return st;
+    if ((st = gemm_t<double2>(ctx, n, wc, n, one, plain(const_cast<double2*>(G2), n), Ub, zero,
+                              RowView<double2>{GU2, 8 * p, nullptr, c0}, tscr)))
+      return st;
+  }
+  for (int c0 = 0; c0 < 4 * p; c0 += 16) {
+    const int wc = min(16, 4 * p - c0);
+    RowView<double2> Vb{V, 4 * p, nullptr, c0};
+    if ((st = gemm_t<double2>(ctx, n, wc, n, one, plain(const_cast<double2*>(H1), n), Vb, zero,
+                              RowView<double2>{HV1, 4 * p, nullptr, c0}, tscr)))
+      return st;
+    if ((st = gemm_t<double2>(ctx, n, wc, n, one, plain(const_cast<double2*>(H2), n), Vb, zero,
+                              RowView<double2>{HV2, 4 * p, nullptr, c0}, tscr)))
+      return st;
+  }
+  opT_combine_kernel<<<ceil_div(4 * np, 256), 256, 0, ctx.stream>>>(n, p, GU1, GU2, HV1, HV2, eps, k0, wv, r);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
 // ------------------------------------------------------------ FP64 operator
 // U = [s | h | e s | e h] (n x 8p) from W = [s | h] (n x 4p)
 __global__ void op_prep_kernel(int n, int p, const double2* __restrict__ W, EpsArg eps, bool second,
@@ -685,6 +959,59 @@ int bem200_bem_precond(int precision, int engine, int n, int npol, void* ws, con
 }
 
 size_t bem200_bem_apply_workspace_size(int n, int npol) { return sizeof(double2) * 40 * (size_t)n * npol; }
+
+size_t bem200_bem_solve_T_workspace_size(int precision, int n, int npol) {
+  const size_t np = (size_t)n * npol;
+  if (precision == 0) return solve_T_scratch_bytes<double2>(n, npol);
+  return align256(solve_T_scratch_bytes<float2>(n, npol)) + 2 * align256(sizeof(float2) * 8 * np) + 256;
+}
+
+int bem200_bem_solve_T(int precision, int engine, int n, int npol, void* ws, const void* cot, int eps_per_face,
+                       const double* eps1, const double* eps2, const double* nvec, double k0, void* b, void* scratch,
+                       void* stream) {
+  BEM_REQUIRE(n > 0 && npol > 0 && ws && cot && b && scratch && eps1 && eps2 && nvec, BEM200_ERR_ARG,
+              "bem_solve_T: bad arguments");
+  BEM_REQUIRE(npol <= 4, BEM200_ERR_UNSUPPORTED, "bem_solve_T: at most 4 polarisations");
+  LaContext ctx;
+  ctx.stream = (cudaStream_t)stream;
+  ctx.engine = engine_from(engine);
+  EpsArg eps = make_eps(eps_per_face, eps1, eps2);
+  const long long np = (long long)n * npol;
+  if (precision == 0)
+    return bem_solve_T_core<double2>(ctx, n, npol, ws, (const double2*)cot, eps, nvec, k0, (double2*)b, scratch);
+  char* p = reinterpret_cast<char*>(scratch);
+  void* core = p;                                   p += align256(solve_T_scratch_bytes<float2>(n, npol));
+  float2* cot32 = reinterpret_cast<float2*>(p);     p += align256(sizeof(float2) * 8 * np);
+  float2* b32 = reinterpret_cast<float2*>(p);       p += align256(sizeof(float2) * 8 * np);
+  unsigned long long* red = reinterpret_cast<unsigned long long*>(p);
+  double cn = 0;
+  int st = absmax_host(ctx.stream, 8 * np, (const double2*)cot, red, &cn);
+  if (st) return st;
+  if (!(cn > 0 && cn < 1e300)) {
+    BEM_CUDA_CHECK(cudaMemsetAsync(b, 0, sizeof(double2) * 8 * np, ctx.stream));
+    return BEM200_OK;
+  }
+  c128_to_c64_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(8 * np, (const double2*)cot, cot32, 1.0 / cn);
+  BEM_LAUNCH_CHECK();
+  if ((st = bem_solve_T_core<float2>(ctx, n, npol, ws, cot32, eps, nvec, k0, b32, core))) return st;
+  axpy_c64_to_c128_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(8 * np, b32, cn, (double2*)b, false);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+size_t bem200_bem_apply_T_workspace_size(int n, int npol) { return apply_T_scratch_bytes(n, npol); }
+
+int bem200_bem_apply_T(int n, int npol, const void* G1, const void* G2, const void* H1, const void* H2,
+                       int eps_per_face, const double* eps1, const double* eps2, const double* nvec, double k0,
+                       const void* l, const void* w, void* r, void* scratch, void* stream) {
+  BEM_REQUIRE(n > 0 && npol > 0 && G1 && G2 && H1 && H2 && l && r && scratch && eps1 && eps2 && nvec,
+              BEM200_ERR_ARG, "bem_apply_T: bad arguments");
+  LaContext ctx;
+  ctx.stream = (cudaStream_t)stream;
+  EpsArg eps = make_eps(eps_per_face, eps1, eps2);
+  return bem_apply_T(ctx, n, npol, (const double2*)G1, (const double2*)G2, (const double2*)H1, (const double2*)H2,
+                     eps, nvec, k0, (const double2*)l, (const double2*)w, (double2*)r, scratch);
+}
 
 int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, const void* G2, const void* H1,
                         const void* H2, const void* b, int eps_per_face, const double* eps1, const double* eps2,

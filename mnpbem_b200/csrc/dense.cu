@@ -1423,6 +1423,12 @@ constexpr long long kSpinLimit = 1LL << 22;
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 template <int B>
 __device__ __forceinline__ void cp_async_elem(void* s, const void* g);
 template <>
@@ -1439,20 +1445,27 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// tile rows [r0, r0 + rb) x columns [c0, c0 + cb) of T -> dst (64 x kTrsvPitch), zero padded
-template <typename C>
+// tile rows [r0, r0 + rb) x columns [c0, c0 + cb) of the operator -> dst (64 x
+// kTrsvPitch), zero padded.  kTrans: the operator is T^T, so dst[r][c] =
+// T(c0 + c, r0 + r); consecutive threads then read consecutive columns of one
+// storage row of T.
+template <typename C, bool kTrans>
 __device__ __forceinline__ void trsv_load_tile(C* dst, const RowView<C>& T, int r0, int rb, int c0, int cb) {
   for (int idx = threadIdx.x; idx < kTrsvBS * kTrsvBS; idx += blockDim.x) {
-    const int r = idx >> 6, c = idx & 63;
+    const int r = kTrans ? (idx & 63) : (idx >> 6), c = kTrans ? (idx >> 6) : (idx & 63);
     C* d = dst + r * kTrsvPitch + c;
     if (r < rb && c < cb)
-      cp_async_elem<sizeof(C)>(d, T.base + T.off(r0 + r, c0 + c));
+      cp_async_elem<sizeof(C)>(d, T.base + (kTrans ? T.off(c0 + c, r0 + r) : T.off(r0 + r, c0 + c)));
     else
       *d = czero<C>();
   }
 }
 
-template <typename C, bool kLower>
+// kLower: forward substitution (blocks depend on earlier blocks), else
+// backward.  kUnit: unit diagonal.  kTrans: the operator is T^T.  The LU
+// factors give (kLower, kUnit) = (true, true) for L and (false, false) for U;
+// their transposes U^T and L^T give (true, false) and (false, true).
+template <typename C, bool kLower, bool kUnit, bool kTrans>
 __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowView<C> T, C* __restrict__ X,
                                                           int* __restrict__ flags, int* __restrict__ ticket,
                                                           int* __restrict__ status) {
@@ -1476,7 +1489,7 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
   auto src_block = [&](int s) { return kLower ? s : nblk - 1 - s; };
   {  // tile 0: the first dependency, or the diagonal block
     const int J = nsrc > 0 ? src_block(0) : I;
-    trsv_load_tile(tiles, T, r0, rb, J * kTrsvBS, min(kTrsvBS, n - J * kTrsvBS));
+    trsv_load_tile<C, kTrans>(tiles, T, r0, rb, J * kTrsvBS, min(kTrsvBS, n - J * kTrsvBS));
     cp_async_commit();
   }
   for (int idx = tid; idx < kTrsvBS * nrhs; idx += 256) {
@@ -1492,19 +1505,21 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
     const int c0 = J * kTrsvBS, cb = min(kTrsvBS, n - c0);
     {  // prefetch tile s + 1 (the next dependency or the diagonal block)
       const int Jn = (s + 1 < nsrc) ? src_block(s + 1) : I;
-      trsv_load_tile(tiles + ((s + 1) & 1) * kTrsvBS * kTrsvPitch, T, r0, rb, Jn * kTrsvBS,
-                     min(kTrsvBS, n - Jn * kTrsvBS));
+      trsv_load_tile<C, kTrans>(tiles + ((s + 1) & 1) * kTrsvBS * kTrsvPitch, T, r0, rb, Jn * kTrsvBS,
+                                 min(kTrsvBS, n - Jn * kTrsvBS));
       cp_async_commit();
     }
     if (tid == 0) {
+      // plain acquire loads: every block waiting on the same flag reads it from
+      // L2 without the serialising read-modify-write of an atomic
       long long spins = 0;
-      while (atomicAdd(&flags[J], 0) == 0) {
+      while (ld_acquire_gpu(&flags[J]) == 0) {
         if (++spins > kSpinLimit) {
           atomicExch(status, BEM200_ERR_TIMEOUT);
           sabort = 1;
           break;
         }
-        __nanosleep(32);
+        if (spins > 16) __nanosleep(32);
       }
       __threadfence();
     }
@@ -1547,22 +1562,31 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
       C x0 = xs[lane * kTrsvMaxRhs + q], x1 = xs[(lane + 32) * kTrsvMaxRhs + q];
       const C* d0 = D + lane * kTrsvPitch;
       const C* d1 = D + (lane + 32) * kTrsvPitch;
+      const C one = cmake<C>(1.0, 0.0);
+      const C inv0 = (!kUnit && lane < rb) ? cdiv(one, d0[lane]) : czero<C>();
+      const C inv1 = (!kUnit && lane + 32 < rb) ? cdiv(one, d1[lane + 32]) : czero<C>();
       if (kLower) {
         for (int r = 0; r < rb; ++r) {
+          if (!kUnit) {
+            if (r < 32) {
+              if (lane == r) x0 = cmul(x0, inv0);
+            } else if (lane == r - 32) {
+              x1 = cmul(x1, inv1);
+            }
+          }
           const C xr = shfl_c(r < 32 ? x0 : x1, r & 31);
           const C u0 = csub(x0, cmul(d0[r], xr)), u1 = csub(x1, cmul(d1[r], xr));
           if (lane > r) x0 = u0;
           if (lane + 32 > r) x1 = u1;
         }
       } else {
-        const C one = cmake<C>(1.0, 0.0);
-        const C inv0 = lane < rb ? cdiv(one, d0[lane]) : czero<C>();
-        const C inv1 = lane + 32 < rb ? cdiv(one, d1[lane + 32]) : czero<C>();
         for (int r = rb - 1; r >= 0; --r) {
-          if (r < 32) {
-            if (lane == r) x0 = cmul(x0, inv0);
-          } else if (lane == r - 32) {
-            x1 = cmul(x1, inv1);
+          if (!kUnit) {
+            if (r < 32) {
+              if (lane == r) x0 = cmul(x0, inv0);
+            } else if (lane == r - 32) {
+              x1 = cmul(x1, inv1);
+            }
           }
           const C xr = shfl_c(r < 32 ? x0 : x1, r & 31);
           const C u0 = csub(x0, cmul(d0[r], xr)), u1 = csub(x1, cmul(d1[r], xr));
@@ -1589,12 +1613,12 @@ static size_t trsv_smem_bytes() {
   return sizeof(C) * (2 * kTrsvBS * kTrsvPitch + 2 * kTrsvBS * kTrsvMaxRhs);
 }
 
-template <typename C, bool kLower>
+template <typename C, bool kLower, bool kUnit = kLower, bool kTrans = false>
 static int trsv_blocked(const LaContext& ctx, int n, int nrhs, RowView<C> T, C* X, int* iscratch) {
   const int nblk = ceil_div(n, kTrsvBS);
   // iscratch: flags [0, nblk), ticket [nblk], local status [nblk + 1]
   BEM_CUDA_CHECK(cudaMemsetAsync(iscratch, 0, sizeof(int) * (nblk + 2), ctx.stream));
-  auto kern = trsv_blocked_kernel<C, kLower>;
+  auto kern = trsv_blocked_kernel<C, kLower, kUnit, kTrans>;
   int st = prep_smem(kern, trsv_smem_bytes<C>());
   if (st) return st;
   kern<<<nblk, 256, trsv_smem_bytes<C>(), ctx.stream>>>(n, nrhs, T, X, iscratch, iscratch + nblk,
@@ -1776,6 +1800,126 @@ int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld,
   return BEM200_OK;
 }
 
+// out[map[i], :] = in[i, :]
+template <typename C>
+__global__ void scatter_rows_kernel(int n, int ncols, const C* __restrict__ in, long long ldi,
+                                    const int32_t* __restrict__ map, C* __restrict__ out, long long ldo) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * ncols) return;
+  int i = (int)(idx / ncols), c = (int)(idx % ncols);
+  out[(long long)map[i] * ldo + c] = in[(long long)i * ldi + c];
+}
+
+// B <- A^-T B: with P A = L U, A^T = U^T L^T P, so U^T y = B (lower, non-unit),
+// L^T u = y (upper, unit), then B[rowmap[i], :] = u[i, :].  nrhs <= 16.
+template <typename C>
+int solve_left_T(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld, const int32_t* rowmap, C* B,
+                 long long ldb, void* scratch) {
+  if (nrhs <= 0) return BEM200_OK;
+  BEM_REQUIRE(scratch, BEM200_ERR_ARG, "solve_left_T: scratch required");
+  BEM_REQUIRE(nrhs <= kTrsvMaxRhs, BEM200_ERR_UNSUPPORTED, "solve_left_T: at most %d right-hand sides", kTrsvMaxRhs);
+  C* Y = reinterpret_cast<C*>(scratch);
+  int* iscr = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) + round256(sizeof(C) * (size_t)n * nrhs));
+  BEM_CUDA_CHECK(cudaMemcpy2DAsync(Y, nrhs * sizeof(C), B, ldb * sizeof(C), nrhs * sizeof(C), n,
+                                   cudaMemcpyDeviceToDevice, ctx.stream));
+  RowView<C> T{const_cast<C*>(LU), ld, rowmap, 0};
+  int st;
+  if ((st = trsv_blocked<C, true, false, true>(ctx, n, nrhs, T, Y, iscr))) return st;
+  if ((st = trsv_blocked<C, false, true, true>(ctx, n, nrhs, T, Y, iscr))) return st;
+  const long long tot = (long long)n * nrhs;
+  scatter_rows_kernel<C><<<ceil_div(tot, 256), 256, 0, ctx.stream>>>(n, nrhs, Y, nrhs, rowmap, B, ldb);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+// Transposed skinny GEMM: Cm (m x w) = alpha A^T B + beta Cm with A (k x m) and
+// B (k x w), w <= W.  Thread t of CTA (x, s) owns column i = 128 x + t of A and
+// the k rows of split s (coalesced row reads of A; the B rows of a 32-row
+// chunk are staged in shared memory); partial sums go to P[s] and a second
+// kernel adds the splits in a fixed order (deterministic).
+constexpr int kSkinnyTCols = 128;
+constexpr int kSkinnyTMaxSplit = 16;
+
+template <typename C, int W>
+__global__ void __launch_bounds__(kSkinnyTCols) gemm_skinny_t_kernel(int m, int w, int k, int kchunk,
+                                                                    RowView<C> A, RowView<C> B,
+                                                                    C* __restrict__ P) {
+  __shared__ C bs[32][W];
+  const int i = blockIdx.x * kSkinnyTCols + threadIdx.x;
+  const int s = blockIdx.y;
+  const int k0 = s * kchunk, k1 = min(k, k0 + kchunk);
+  C acc[W];
+#pragma unroll
+  for (int q = 0; q < W; ++q) acc[q] = czero<C>();
+  for (int kb = k0; kb < k1; kb += 32) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 32 * W; idx += kSkinnyTCols) {
+      const int r = idx / W, q = idx % W;
+      bs[r][q] = (kb + r < k1 && q < w) ? B.at(kb + r, q) : czero<C>();
+    }
+    __syncthreads();
+    const int nr = min(32, k1 - kb);
+    if (i < m) {
+      for (int r = 0; r < nr; ++r) {
+        const C a = A.at(kb + r, i);
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          const C b = bs[r][q];
+          acc[q].x = fma(a.x, b.x, acc[q].x);
+          acc[q].x = fma(-a.y, b.y, acc[q].x);
+          acc[q].y = fma(a.x, b.y, acc[q].y);
+          acc[q].y = fma(a.y, b.x, acc[q].y);
+        }
+      }
+    }
+  }
+  if (i < m) {
+#pragma unroll
+    for (int q = 0; q < W; ++q)
+      if (q < w) P[((long long)s * m + i) * w + q] = acc[q];
+  }
+}
+
+template <typename C>
+__global__ void skinny_t_reduce_kernel(int m, int w, int nsplit, const C* __restrict__ P, C alpha, C beta,
+                                       RowView<C> Cv) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)m * w) return;
+  const int i = (int)(idx / w), q = (int)(idx % w);
+  C acc = czero<C>();
+  for (int s = 0; s < nsplit; ++s) acc = cadd(acc, P[(long long)s * m * w + idx]);
+  C v = cmul(alpha, acc);
+  C& out = Cv.at(i, q);
+  if (beta.x != 0 || beta.y != 0) v = cadd(v, cmul(beta, out));
+  out = v;
+}
+
+template <typename C>
+size_t gemm_t_scratch_bytes(int m, int w) {
+  return round256(sizeof(C) * (size_t)kSkinnyTMaxSplit * m * w);
+}
+
+template <typename C>
+int gemm_t(const LaContext& ctx, int m, int w, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv,
+           void* scratch) {
+  if (m <= 0 || w <= 0) return BEM200_OK;
+  BEM_REQUIRE(w <= 16 && scratch, BEM200_ERR_UNSUPPORTED, "gemm_t: at most 16 columns and a scratch buffer");
+  const int ncol = ceil_div(m, kSkinnyTCols);
+  const int nsplit = max(1, min(kSkinnyTMaxSplit, ceil_div(4 * 148, ncol)));
+  const int kchunk = ceil_div(k, nsplit);
+  C* P = reinterpret_cast<C*>(scratch);
+  dim3 grid(ncol, nsplit);
+  if (w <= 8)
+    gemm_skinny_t_kernel<C, 8><<<grid, kSkinnyTCols, 0, ctx.stream>>>(m, w, k, kchunk, A, B, P);
+  else
+    gemm_skinny_t_kernel<C, 16><<<grid, kSkinnyTCols, 0, ctx.stream>>>(m, w, k, kchunk, A, B, P);
+  BEM_LAUNCH_CHECK();
+  skinny_t_reduce_kernel<C><<<ceil_div((long long)m * w, 256), 256, 0, ctx.stream>>>(m, w, nsplit, P, alpha, beta,
+                                                                                       Cv);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
 template <typename C>
 static int solve_right_rows(const LaContext& ctx, int n, int m, const C* LU, long long ld, const int32_t* rowmap,
                             C* X, long long ldx, C* tmp);
@@ -1863,7 +2007,11 @@ int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_
   template int solve_left<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long,     \
                              void*);                                                                             \
   template int solve_right<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long, C*); \
-  template int inverse<C>(const LaContext&, int, const C*, long long, const int32_t*, C*, long long);
+  template int inverse<C>(const LaContext&, int, const C*, long long, const int32_t*, C*, long long);         \
+  template int solve_left_T<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long,   \
+                               void*);                                                                           \
+  template size_t gemm_t_scratch_bytes<C>(int, int);                                                             \
+  template int gemm_t<C>(const LaContext&, int, int, int, C, RowView<C>, RowView<C>, C, RowView<C>, void*);
 BEM_INST(double2)
 BEM_INST(float2)
 

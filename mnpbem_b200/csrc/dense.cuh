@@ -128,6 +128,20 @@ template <typename C>
 int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld, const int32_t* rowmap, C* B,
                long long ldb, void* scratch);
 
+// B <- A^-T B for the factor (LU, rowmap) (transposed solve, nrhs <= 16);
+// scratch: solve_left_scratch_bytes.
+template <typename C>
+int solve_left_T(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld, const int32_t* rowmap, C* B,
+                 long long ldb, void* scratch);
+
+// Cm (m x w) = alpha A^T B + beta Cm, A (k x m), B (k x w), w <= 16;
+// scratch: gemm_t_scratch_bytes(m, w).  Deterministic (fixed summation order).
+template <typename C>
+size_t gemm_t_scratch_bytes(int m, int w);
+template <typename C>
+int gemm_t(const LaContext& ctx, int m, int w, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv,
+           void* scratch);
+
 // X <- X A^-1 (X is m x n); tmp: m x n elements.
 template <typename C>
 int solve_right(const LaContext& ctx, int n, int m, const C* LU, long long ld, const int32_t* rowmap, C* X,

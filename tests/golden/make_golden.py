@@ -34,12 +34,14 @@ input/output vectors that pin the oracle and the geometry module:
                           and the parameters of its preset Drude metals.
 * ``planewave_field.npz`` : PlaneWaveRet.field of the reference on a small curved rod.
 * ``editing.npz``       : Particle.rot and ComParticle shift / scale / rot / ipart of the reference.
+* ``shape_fd_rod.npz``  : the reference solver's central-difference derivatives of the extinction
+                          of a small curved rod along seeded vertex directions (h = 1e-4 nm).
 * ``field_potential.npz`` : BEMRet.potential / .field inside and outside and slices of the
                           Cartesian-derivative Green functions (Gp, H1p, H2p) of the small dimer
                           (two polarisations) and the vacuum sphere.
 
 Usage:  MNPBEM_REFERENCE=<reference checkout> python tests/golden/make_golden.py [--skip-cfg1] [--hmat-only]
-        [--meshes-only] [--field-only]
+        [--meshes-only] [--field-only] [--shape-only]
 """
 import os
 import sys
@@ -288,6 +290,41 @@ def field_potential():
     save("field_potential.npz", **out)
 
 
+def shape_fd():
+    """The reference solver's own finite-difference derivatives of the
+    extinction with respect to the vertices: trirod(12, 30, [9, 5, 5]) curved
+    (96 faces, triangles and quads), gold in eps 1.77, 640 nm, x-polarised;
+    central differences with step h = 1e-4 nm of the unmodified BEMRet along
+    4 seeded unit directions in the space of the particle's verts2 (the nodes
+    that fix the curved geometry; corner vertices stay, as in
+    mnpbem_b200.shape.perturbed)."""
+    from mnpbem.geometry import trirod
+
+    def build(delta):
+        part = trirod(12.0, 30.0, [9, 5, 5], interp="curv")
+        if delta is not None:
+            part.verts2 = part.verts2 + delta
+            part._norm()
+        return ComParticle([EpsConst(1.77), EpsDrude(*DRUDE_AU)], [part], [[2, 1]], 1, interp="curv")
+
+    p0 = build(None)
+    v2 = p0.p[0].verts2.copy()
+    rng = np.random.default_rng(11)
+    D = rng.standard_normal((4,) + v2.shape)
+    D /= np.sqrt(np.sum(D * D, axis=(1, 2), keepdims=True))
+    h, enei = 1e-4, 640.0
+    exc = PlaneWaveRet(POL, DIR)
+
+    def ext_of(p):
+        bem = BEMRet(p)
+        sig, _ = bem.solve(exc.potential(p, enei))
+        return exc.extinction(sig)
+
+    ext0 = ext_of(p0)
+    dext = np.array([(ext_of(build(h * d)) - ext_of(build(-h * d))) / (2 * h) for d in D])
+    save("shape_fd_rod.npz", verts2=v2, D=D, h=h, enei=enei, ext=ext0, dext=dext)
+
+
 def hmat_trees():
     """Cluster trees, block partitions and ACA ranks of the reference H-matrix
     (mnpbem/greenfun/clustertree.py, hmatrix.py) for the sphere (cleaf 32,
@@ -391,6 +428,9 @@ if __name__ == "__main__":
     if "--field-only" in sys.argv:
         field_potential()
         sys.exit(0)
+    if "--shape-only" in sys.argv:
+        shape_fd()
+        sys.exit(0)
     if "--meshes-only" in sys.argv:
         meshes()
         matlab_rod()
@@ -415,5 +455,6 @@ if __name__ == "__main__":
     dimer_small()
     matlab_cfg0()
     field_potential()
+    shape_fd()
     if "--skip-cfg1" not in sys.argv:
         dimer_cfg1()
