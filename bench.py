@@ -246,6 +246,7 @@ def run_ours(args):
         torch.cuda.empty_cache()
 
     roof = roofline_gemm(dev) if rank == 0 else None
+    fp64_tf = fp64_peak(dev) if (rank == 0 and fp64_rate) else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cp)
@@ -279,6 +280,12 @@ def run_ours(args):
             "ext_650nm": ext650,
             "ext_rel_err_vs_reference_fp64": ext_err,
             "fp64_solves_per_s": round(fp64_rate, 4) if fp64_rate else None,
+            "fp64_path_roofline": {
+                "achieved_tflops": round(32.0 * cp.n ** 3 * fp64_rate / 1e12, 3),
+                "peak_tflops": round(fp64_tf, 2),
+                "peak_source": "cuBLAS DGEMM 4096^3 measured in this run (FP64 yardstick)",
+                "frac": round(32.0 * cp.n ** 3 * fp64_rate / 1e12 / fp64_tf, 4),
+            } if (fp64_rate and fp64_tf) else None,
             "mixed_over_fp64": round(value / fp64_rate, 3) if fp64_rate else None,
             "l2": "working set 2.1 GB of complex128 matrices per step (>> 126 MB L2); no flush needed",
             "parallelism": "replicas x{}".format(world),
@@ -350,6 +357,26 @@ def roofline_gemm(dev):
             "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch",
             "algorithmic_flops_per_launch": 8.0 * m * n * k, "shape": [m, n, k], "ms_per_launch": round(1e3 * t, 3),
             "peak_sustained": peak_s, "peak_sustained_source": src_s}
+
+
+def fp64_peak(dev):
+    """FP64 yardstick of this GPU: cuBLAS DGEMM (torch.matmul, 4096^3) timed
+    with CUDA events -- the denominator of the FP64 path's roofline fraction
+    (the FP64 path runs its complex128 GEMMs on CUDA cores)."""
+    import torch
+    n = 4096
+    A = torch.randn(n, n, dtype=torch.float64, device=dev)
+    B = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(A, B)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        torch.matmul(A, B)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / 5
+    return 2.0 * n ** 3 / t / 1e12
 
 
 def cpu_model():

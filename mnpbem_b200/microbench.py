@@ -10,6 +10,7 @@
     python -m mnpbem_b200.microbench sweep [--seed 0] [--nlambda 128] [--workers 4] [--schedule interleave|mesh]
     python -m mnpbem_b200.microbench shape [--nlambda 5] [--ndir 32] [--check 4] [--precision mixed]
     python -m mnpbem_b200.microbench peaks [--m 8192] [--reps 5]
+    python -m mnpbem_b200.microbench vgrad [--shape rod|cube] [--nlambda 5] [--check 2] [--precision mixed]
 
 ``step`` runs whole per-wavelength solves (assembly + init + solve) of the
 sphere dimer (two trisphere(faces) spheres, 2 nm gap, water, Drude gold,
@@ -354,6 +355,58 @@ def case_shape(a):
             "max_mem_GB": torch.cuda.max_memory_allocated() / 1e9}
 
 
+def case_vgrad(a):
+    """Reverse-mode gradient of the extinction over every vertex coordinate
+    (one transposed solve with the wavelength's factors, the operator
+    derivative contracted on the GPU): the gold rod trirod(20, 80, [41, 16,
+    31]) (2400 curved faces, eps_b 1.77) at nlambda wavelengths 600-800 nm,
+    or with --shape cube the rounded gold cube tricube(66, 100 nm, e = 0.25)
+    (25344 curved quads, vacuum) at 700 nm.  ``check`` seeded directions at
+    the first wavelength are compared with central differences of full fp64
+    solves (step 1e-4 nm)."""
+    import torch
+    from . import BEMRet, ComParticle, EpsConst, EpsDrude, PlaneWaveRet
+    from .geometry import tricube, trirod
+    from .shape import extinction_vertex_vjp, perturbed, random_directions
+    if a.shape == "cube":
+        cp = ComParticle([EpsConst(1.0), EpsDrude(9.84, 9.0, 0.067)],
+                         [tricube(a.cube_n, 100.0, a.cube_e, interp="curv")], [[2, 1]], 1, interp="curv")
+        enei = np.array([700.0])
+    else:
+        cp = ComParticle([EpsConst(1.77), EpsDrude(9.84, 9.0, 0.067)],
+                         [trirod(20.0, 80.0, [41, 16, 31], interp="curv")], [[2, 1]], 1, interp="curv")
+        enei = np.linspace(600.0, 800.0, a.nlambda)
+    exc = PlaneWaveRet(np.array([[1.0, 0, 0]]), np.array([[0, 0, 1.0]]))
+    bem = BEMRet(cp, precision=a.precision)
+    t_init, t_grad, exts, grads = [], [], [], []
+    for e in enei:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bem.init(float(e))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        ext, g = extinction_vertex_vjp(bem, exc, float(e))
+        torch.cuda.synchronize()
+        t_init.append(t1 - t0)
+        t_grad.append(time.perf_counter() - t1)
+        exts.append(float(ext[0]))
+        grads.append(g)
+    worst = 0.0
+    D = random_directions(cp, max(a.check, 1), seed=a.seed)
+    for k in range(a.check):
+        e2 = []
+        for s in (1.0, -1.0):
+            q = perturbed(cp, s * 1e-4 * D[k])
+            e2.append(float(BEMRet(q).cross_sections(exc, float(enei[0]))["ext"][0]))
+        fd = (e2[0] - e2[1]) / 2e-4
+        got = float(np.sum(grads[0] * D[k]))
+        worst = max(worst, abs(got - fd) / max(abs(fd), 1e-12))
+    return {"case": "vgrad", "shape": a.shape, "faces": cp.n, "nvert": int(grads[0].shape[0]),
+            "precision": a.precision, "enei": enei.tolist(), "ext": exts, "s_init_per_lambda": t_init,
+            "s_solve_adjoint_gradient_per_lambda": t_grad, "fd_checked": a.check, "max_fd_relerr": worst,
+            "max_mem_GB": torch.cuda.max_memory_allocated() / 1e9}
+
+
 def case_peaks(a):
     """Reference pipe rates of this GPU, from cuBLAS through torch.matmul
     (library GEMMs used only as a yardstick): FP64 (DGEMM, ZGEMM), FP32
@@ -386,7 +439,7 @@ def case_peaks(a):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter", "large", "sweep",
-                                           "shape", "peaks"])
+                                           "shape", "peaks", "vgrad"])
     ap.add_argument("--faces", type=int, default=1444)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--engine", type=int, default=1)
@@ -405,7 +458,7 @@ def main(argv=None):
     ap.add_argument("--hmatrix", action="store_true")
     ap.add_argument("--noprecond", action="store_true")
     ap.add_argument("--side", type=int, default=3)
-    ap.add_argument("--shape", default="spheres", choices=["spheres", "cube"])
+    ap.add_argument("--shape", default="spheres", choices=["spheres", "cube", "rod"])
     ap.add_argument("--cube-n", dest="cube_n", type=int, default=66)
     ap.add_argument("--cube-e", dest="cube_e", type=float, default=0.25)
     ap.add_argument("--seed", type=int, default=0)
@@ -423,7 +476,7 @@ def main(argv=None):
         a.engine = {0: "simt", 1: "bf16x3"}[a.engine]
     out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf, "hmat": case_hmat,
            "iter": case_iter, "large": case_large, "sweep": case_sweep,
-           "shape": case_shape, "peaks": case_peaks}[a.case](a)
+           "shape": case_shape, "peaks": case_peaks, "vgrad": case_vgrad}[a.case](a)
     print(json.dumps(out), flush=True)
 
 
