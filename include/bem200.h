@@ -210,12 +210,13 @@ size_t bem200_gemm_workspace_size(int engine, int m, int n, int k);
  * use partial pivoting.  Replaces the LU factorisations of BEMRet.init
  * (mnpbem/bem/bem_ret.py:437-523, via mnpbem/utils/gpu.py:145).
  * bem200_getrf_ex: flags BEM200_GETRF_PARTIAL_PIVOTING = partial pivoting
- * for complex64 too. */
+ * for complex64 too; lookahead_nb = block width of the look-ahead schedule
+ * (multiple of 32 in [64, 1024]; 0 = 128). */
 #define BEM200_GETRF_PARTIAL_PIVOTING 1
 int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
                  int32_t* info, void* ws, size_t ws_bytes, void* stream);
 int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
-                    int32_t* info, void* ws, size_t ws_bytes, int flags, void* stream);
+                    int32_t* info, void* ws, size_t ws_bytes, int flags, int lookahead_nb, void* stream);
 /* ws of this size lets bem200_getrf run its look-ahead schedule: panels on a
  * high-priority stream, trailing updates on a low-priority one, both forked
  * from and joined back into `stream` (same pivots and factors).  A smaller
@@ -269,6 +270,13 @@ int bem200_bem_slots(int precision, int n, void* ws, void** G1, void** G2, void*
 int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face, const double* eps1,
                     const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
                     int32_t* info_host, void* stream);
+/* bem200_bem_init with the LU tiling exposed (for the project's autotuner):
+ * lu_flags BEM200_GETRF_PARTIAL_PIVOTING (complex64 factors with partial
+ * pivoting instead of tournament panels), lookahead_nb the block width of the
+ * look-ahead LU schedule (a multiple of 32 in [64, 1024]; 0 = 128). */
+int bem200_bem_init_ex(int precision, int engine, int n, void* ws, int eps_per_face, const double* eps1,
+                       const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
+                       int lu_flags, int lookahead_nb, int32_t* info_host, void* stream);
 
 /* Right-hand side (complex128, row-major, npol polarisations):
  *   b = [phi (n, p) | a (n, 3, p) | alpha (n, 3, p) | De (n, p)]  (8 n p values)

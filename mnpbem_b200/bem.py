@@ -82,7 +82,7 @@ class BEMRet:
     needs = {"sim": "ret"}
 
     def __init__(self, p, enei=None, precision="fp64", engine="bf16x3", ir_tol=1e-12, ir_maxit=30, gmres_ir=True,
-                 gmres_maxit=200, **options):
+                 gmres_maxit=200, lu_tiles=None, **options):
         torch = _torch()
         if p is None:
             raise ValueError("BEMRet: 'p' must be a ComParticle (or compatible particle object), got None.")
@@ -102,6 +102,10 @@ class BEMRet:
         self.ir_maxit = int(ir_maxit)
         self.gmres_ir = bool(gmres_ir)
         self.gmres_maxit = int(gmres_maxit)
+        if not (lu_tiles is None or lu_tiles == "auto" or (isinstance(lu_tiles, int) and lu_tiles % 32 == 0
+                                                           and 64 <= lu_tiles <= 1024)):
+            raise ValueError("BEMRet: lu_tiles must be None, 'auto' or a look-ahead width (multiple of 32, 64-1024)")
+        self.lu_tiles = lu_tiles
         self.options = dict(options)
         self.enei = None
         self.dev = torch.device("cuda")
@@ -173,11 +177,25 @@ class BEMRet:
             for src, dst in zip(self._G128, self._slots):
                 nat.call("bem200_convert_c128_c64", n * n, nat.ptr(src), ctypes.c_void_p(dst), s)
         info = ctypes.c_int32(0)
-        nat.call("bem200_bem_init", self._prec, _ENGINES[self.engine], n, nat.ptr(self._ws), self._eps_mode,
-                 self._e1p, self._e2p, nat.ptr(self._nvec), self.k, nat.ptr(self._gws), self._gws_bytes,
-                 ctypes.byref(info), s)
+        nat.call("bem200_bem_init_ex", self._prec, _ENGINES[self.engine], n, nat.ptr(self._ws), self._eps_mode,
+                 self._e1p, self._e2p, nat.ptr(self._nvec), self.k, nat.ptr(self._gws), self._gws_bytes, 0,
+                 self._lookahead(), ctypes.byref(info), s)
         self.enei = enei
         return self
+
+    def _lookahead(self):
+        """Look-ahead block width of the LU factorisations (0: the library's
+        default); 'auto' measures it once per size on this GPU
+        (mnpbem_b200.tuning, cached)."""
+        if self.lu_tiles is None:
+            return 0
+        if self.lu_tiles == "auto":
+            if getattr(self, "_la_tuned", None) is None:
+                from .tuning import tune_lookahead
+                self._la_tuned, _ = tune_lookahead(self.n, "c128" if self._prec == 0 else "c64",
+                                                   _ENGINES[self.engine])
+            return self._la_tuned
+        return int(self.lu_tiles)
 
     def _assemble_into_slots(self, enei, dtype):
         g = self.g

@@ -775,15 +775,19 @@ int bem200_bem_slots(int precision, int n, void* ws, void** G1, void** G2, void*
   return BEM200_OK;
 }
 
-int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face, const double* eps1,
-                    const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
-                    int32_t* info_host, void* stream) {
+int bem200_bem_init_ex(int precision, int engine, int n, void* ws, int eps_per_face, const double* eps1,
+                       const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
+                       int lu_flags, int lookahead_nb, int32_t* info_host, void* stream) {
   BEM_REQUIRE(n > 0 && ws && eps1 && eps2 && nvec, BEM200_ERR_ARG, "bem_init: bad arguments");
+  BEM_REQUIRE((lu_flags & ~BEM200_GETRF_PARTIAL_PIVOTING) == 0, BEM200_ERR_ARG, "bem_init: unknown LU flags 0x%x",
+              lu_flags);
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
   ctx.engine = engine_from(engine);
   ctx.ws = gemm_ws;
   ctx.ws_bytes = gemm_ws_bytes;
+  ctx.tournament = (lu_flags & BEM200_GETRF_PARTIAL_PIVOTING) == 0;
+  ctx.la_nb = lookahead_nb;
   EpsArg eps = make_eps(eps_per_face, eps1, eps2);
   int st = precision == 0 ? bem_init_t<double2>(ctx, n, ws, eps, nvec, k0) : bem_init_t<float2>(ctx, n, ws, eps, nvec, k0);
   if (st) return st;
@@ -794,6 +798,13 @@ int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face
     BEM_REQUIRE(*info_host == 0, BEM200_ERR_SINGULAR, "bem_init: exactly singular pivot at column %d", *info_host);
   }
   return BEM200_OK;
+}
+
+int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face, const double* eps1,
+                    const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
+                    int32_t* info_host, void* stream) {
+  return bem200_bem_init_ex(precision, engine, n, ws, eps_per_face, eps1, eps2, nvec, k0, gemm_ws, gemm_ws_bytes, 0, 0,
+                            info_host, stream);
 }
 
 size_t bem200_bem_solve_workspace_size(int precision, int n, int npol) {

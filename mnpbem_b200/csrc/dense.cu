@@ -1650,18 +1650,22 @@ static int getrf_rec(const LaContext& ctx, int n, C* A, long long ld, int32_t* r
   return getrf_rec(ctx, n, A, ld, rowmap, ipiv, col0 + w1, w - w1);
 }
 
-// Blocked right-looking LU with look-ahead (block columns of kLaNB).  Step j:
+// Blocked right-looking LU with look-ahead (block columns of ctx.la_nb, a
+// multiple of 32; 128 by default, tunable per size).  Step j:
 //   panel(j)   : getrf_rec on block column j                [high-priority stream]
 //   narrow(j)  : U(j, j+1) = L(j,j)^-1 A(j, j+1) and the update of block
 //                column j+1 -- all the next panel needs     [high-priority stream]
 //   wide(j)    : the same for block columns j+2..           [low-priority stream]
 // so the wide TRSM + tensor-core GEMM of step j runs while panel(j+1) is
 // factored.  narrow(j) waits for wide(j-1), wide(j) waits for panel(j).
-// panel(j+1) permutes logical rows >= (j+1) kLaNB while wide(j) updates them,
+// panel(j+1) permutes logical rows >= (j+1) nb while wide(j) updates them,
 // so wide(j) addresses those rows through a snapshot of the row map taken
 // right after panel(j) (two snapshots alternate).  The rows themselves never
 // move, so both orders give the same matrix.
-constexpr int kLaNB = 128;
+static int la_width(const LaContext& ctx) {
+  const int w = ctx.la_nb > 0 ? ctx.la_nb : 128;
+  return max(64, min(1024, (w / kPanelNB) * kPanelNB));
+}
 
 struct LaStreams {
   cudaStream_t hi = nullptr, lo = nullptr;
@@ -1701,12 +1705,13 @@ static int getrf_lookahead(const LaContext& ctx, int n, C* A, long long ld, int3
   BEM_LAUNCH_CHECK();
   bool wide_pending = false;
   int st;
-  for (int c0 = 0, j = 0; c0 < n; c0 += kLaNB, ++j) {
-    const int w = min(kLaNB, n - c0);
+  const int nb = la_width(ctx);
+  for (int c0 = 0, j = 0; c0 < n; c0 += nb, ++j) {
+    const int w = min(nb, n - c0);
     if ((st = getrf_rec(cm, n, A, ld, rowmap, ipiv, c0, w))) return st;
     const int c1 = c0 + w;
     if (c1 >= n) break;
-    const int w1 = min(kLaNB, n - c1), c2 = c1 + w1;
+    const int w1 = min(nb, n - c1), c2 = c1 + w1;
     int32_t* sn = snap + (size_t)(j & 1) * n;  // sn[i] = rowmap[c1 + i] as of the end of panel(j)
     if (c2 < n) {
       BEM_CUDA_CHECK(cudaMemcpyAsync(sn, rowmap + c1, sizeof(int32_t) * (n - c1), cudaMemcpyDeviceToDevice, ls.hi));
@@ -1741,8 +1746,8 @@ int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int3
   // look-ahead needs the row-map snapshots (scratch) and, on the tensor-core
   // engines, room for two concurrent GEMMs in the operand workspace
   const bool ws_ok = ctx.engine == GemmEngine::kSimt ||
-                     gemm_tc_workspace(n, n, kLaNB, ctx.engine) <= ((ctx.ws_bytes / 2) & ~size_t(255));
-  if (scratch && n > 2 * kLaNB && ws_ok) return getrf_lookahead<C>(ctx, n, A, ld, rowmap, ipiv, scratch);
+                     gemm_tc_workspace(n, n, la_width(ctx), ctx.engine) <= ((ctx.ws_bytes / 2) & ~size_t(255));
+  if (scratch && n > 2 * la_width(ctx) && ws_ok) return getrf_lookahead<C>(ctx, n, A, ld, rowmap, ipiv, scratch);
   iota_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(n, rowmap);
   BEM_LAUNCH_CHECK();
   return getrf_rec(ctx, n, A, ld, rowmap, ipiv, 0, n);
@@ -2061,7 +2066,7 @@ size_t bem200_getrf_workspace_size(int dtype, int engine, int n) {
 }
 
 int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv, int32_t* info,
-                    void* ws, size_t ws_bytes, int flags, void* stream) {
+                    void* ws, size_t ws_bytes, int flags, int lookahead_nb, void* stream) {
   BEM_REQUIRE((flags & ~BEM200_GETRF_PARTIAL_PIVOTING) == 0, BEM200_ERR_ARG, "getrf: unknown flags 0x%x", flags);
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
@@ -2070,6 +2075,7 @@ int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* 
   ctx.ws_bytes = ws_bytes;
   ctx.dinfo = info;
   ctx.tournament = (flags & BEM200_GETRF_PARTIAL_PIVOTING) == 0;
+  ctx.la_nb = lookahead_nb;
   int32_t* snap = nullptr;
   if (ws && n > 0 && ws_bytes >= bem200_getrf_workspace_size(dtype, engine, n)) {
     const size_t sb = getrf_snap_bytes(n);
@@ -2084,7 +2090,7 @@ int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* 
 
 int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv, int32_t* info,
                  void* ws, size_t ws_bytes, void* stream) {
-  return bem200_getrf_ex(dtype, engine, n, A, ld, rowmap, ipiv, info, ws, ws_bytes, 0, stream);
+  return bem200_getrf_ex(dtype, engine, n, A, ld, rowmap, ipiv, info, ws, ws_bytes, 0, 0, stream);
 }
 
 size_t bem200_getrs_workspace_size(int dtype, int n, int nrhs) {

@@ -129,7 +129,7 @@ def case_getrf(a):
     def go():
         A.copy_(A0)
         nat.call("bem200_getrf_ex", code, a.engine, n, nat.ptr(A), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info),
-                 nat.ptr(ws), wsb, flags, nat.stream_ptr())
+                 nat.ptr(ws), wsb, flags, a.la_nb, nat.stream_ptr())
     go()
     # backward error of a solve with these factors: |A0 x - b| / (|A0| |x|)
     b = torch.randn(n, 2, dtype=dt, device="cuda", generator=gen)
@@ -452,6 +452,7 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--graph", action="store_true", help="getrf: replay from a CUDA graph")
     ap.add_argument("--partial", action="store_true", help="getrf: partial pivoting for complex64 too")
+    ap.add_argument("--la-nb", dest="la_nb", type=int, default=0, help="getrf: look-ahead block width (0 = 128)")
     ap.add_argument("--cleaf", type=int, default=200)
     ap.add_argument("--htol", type=float, default=1e-6)
     ap.add_argument("--tol", type=float, default=1e-10)

@@ -207,7 +207,7 @@ def test_getrf_c64_tournament_pivoting(cuda, n):
         wsb = int(nat.lib().bem200_getrf_workspace_size(nat.C64, 1, n))
         ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
         nat.call("bem200_getrf_ex", nat.C64, 1, n, nat.ptr(At), n, nat.ptr(rowmap), nat.ptr(ipiv), nat.ptr(info),
-                 nat.ptr(ws), wsb, flags, nat.stream_ptr())
+                 nat.ptr(ws), wsb, flags, 0, nat.stream_ptr())
         assert int(info.item()) == 0
         perm = rowmap.cpu().numpy()
         assert sorted(perm.tolist()) == list(range(n))      # a permutation
