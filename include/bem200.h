@@ -273,10 +273,13 @@ int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face
 /* bem200_bem_init with the LU tiling exposed (for the project's autotuner):
  * lu_flags BEM200_GETRF_PARTIAL_PIVOTING (complex64 factors with partial
  * pivoting instead of tournament panels), lookahead_nb the block width of the
- * look-ahead LU schedule (a multiple of 32 in [64, 1024]; 0 = 128). */
+ * look-ahead LU schedule (a multiple of 32 in [64, 1024]; 0 = 128).
+ * phase_ms (HOST, 4 floats, or NULL): stage timer (CUDA events on the
+ * stream; the call then synchronises): LU(G1) || LU(G2) with Sigma1 || Sigma2,
+ * LU(Delta), Delta^-1, Sigma build + LU(Sigma). */
 int bem200_bem_init_ex(int precision, int engine, int n, void* ws, int eps_per_face, const double* eps1,
                        const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
-                       int lu_flags, int lookahead_nb, int32_t* info_host, void* stream);
+                       int lu_flags, int lookahead_nb, float* phase_ms, int32_t* info_host, void* stream);
 
 /* Right-hand side (complex128, row-major, npol polarisations):
  *   b = [phi (n, p) | a (n, 3, p) | alpha (n, 3, p) | De (n, p)]  (8 n p values)

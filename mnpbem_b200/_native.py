@@ -74,7 +74,7 @@ _SIGS = {
     "bem200_bem_init": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp,
                                        _dbl, _vp, _sz, _vp, _vp]),
     "bem200_bem_init_ex": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp,
-                                          _dbl, _vp, _sz, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+                                          _dbl, _vp, _sz, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "bem200_bem_solve_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "bem200_bem_solve": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp,
                                         _vp, ctypes.c_int, _vp, _vp, _vp, _dbl, _vp, _vp, _vp, _vp, _sz, _vp]),

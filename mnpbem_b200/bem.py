@@ -106,6 +106,9 @@ class BEMRet:
                                                            and 64 <= lu_tiles <= 1024)):
             raise ValueError("BEMRet: lu_tiles must be None, 'auto' or a look-ahead width (multiple of 32, 64-1024)")
         self.lu_tiles = lu_tiles
+        # stage timer of init (profiling): set to (ctypes.c_float * 4)() to record the phases
+        self._phase_buf = None
+        self.last_init_phases_ms = None
         self.options = dict(options)
         self.enei = None
         self.dev = torch.device("cuda")
@@ -179,7 +182,9 @@ class BEMRet:
         info = ctypes.c_int32(0)
         nat.call("bem200_bem_init_ex", self._prec, _ENGINES[self.engine], n, nat.ptr(self._ws), self._eps_mode,
                  self._e1p, self._e2p, nat.ptr(self._nvec), self.k, nat.ptr(self._gws), self._gws_bytes, 0,
-                 self._lookahead(), ctypes.byref(info), s)
+                 self._lookahead(), self._phase_buf, ctypes.byref(info), s)
+        if self._phase_buf is not None:
+            self.last_init_phases_ms = list(self._phase_buf)
         self.enei = enei
         return self
 

@@ -122,15 +122,31 @@ struct ForkJoin {
   }
 };
 
+// Optional CUDA-event stage timer of the init: events at the start and after
+// each phase, recorded on the caller's stream.
+struct StageTimer {
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  ~StageTimer() {
+    for (cudaEvent_t& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
 template <typename C>
-static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, const double* nvec, double k0) {
+static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, const double* nvec, double k0,
+                      StageTimer* tm = nullptr) {
   BemState<C> s = state_view<C>(n, ws);
+  auto mark = [&](int i) -> int {
+    if (tm) BEM_CUDA_CHECK(cudaEventRecord(tm->ev[i], ctx.stream));
+    return BEM200_OK;
+  };
   const long long nn = (long long)n * n;
   LaContext c = ctx;
   c.dinfo = s.info;
   c.dstatus = s.status;
   BEM_CUDA_CHECK(cudaMemsetAsync(s.info, 0, 2 * sizeof(int), ctx.stream));
   int st;
+  if ((st = mark(0))) return st;
   // a second chain needs half of the operand workspace for the largest GEMM of
   // an LU / right solve (n x n/2 x n/2, rounded up)
   const int half = n / 2 + 64;
@@ -163,16 +179,19 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
     BEM_CUDA_CHECK(cudaStreamWaitEvent(ctx.stream, fj.join, 0));
     c.ws_bytes = ctx.ws_bytes;
   }
+  if ((st = mark(1))) return st;
   // Delta = Sigma1 - Sigma2, LU(Delta), Delta^-1
   delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[4]);
   BEM_LAUNCH_CHECK();
   if ((st = getrf<C>(c, n, s.M[4], n, s.map[2], s.ipiv[2], s.snap[0]))) return st;
+  if ((st = mark(2))) return st;
   if ((st = inverse<C>(c, n, s.M[4], n, s.map[2], s.M[5], n))) return st;
+  if ((st = mark(3))) return st;
   // Sigma, LU(Sigma)
   sigma_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(n, s.M[2], s.M[3], s.M[5], nvec, eps, k0 * k0, s.M[6]);
   BEM_LAUNCH_CHECK();
   if ((st = getrf<C>(c, n, s.M[6], n, s.map[3], s.ipiv[3], s.snap[0]))) return st;
-  return BEM200_OK;
+  return mark(4);
 }
 
 // ------------------------------------------------------------ solve kernels
@@ -777,7 +796,7 @@ int bem200_bem_slots(int precision, int n, void* ws, void** G1, void** G2, void*
 
 int bem200_bem_init_ex(int precision, int engine, int n, void* ws, int eps_per_face, const double* eps1,
                        const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
-                       int lu_flags, int lookahead_nb, int32_t* info_host, void* stream) {
+                       int lu_flags, int lookahead_nb, float* phase_ms, int32_t* info_host, void* stream) {
   BEM_REQUIRE(n > 0 && ws && eps1 && eps2 && nvec, BEM200_ERR_ARG, "bem_init: bad arguments");
   BEM_REQUIRE((lu_flags & ~BEM200_GETRF_PARTIAL_PIVOTING) == 0, BEM200_ERR_ARG, "bem_init: unknown LU flags 0x%x",
               lu_flags);
@@ -789,8 +808,17 @@ int bem200_bem_init_ex(int precision, int engine, int n, void* ws, int eps_per_f
   ctx.tournament = (lu_flags & BEM200_GETRF_PARTIAL_PIVOTING) == 0;
   ctx.la_nb = lookahead_nb;
   EpsArg eps = make_eps(eps_per_face, eps1, eps2);
-  int st = precision == 0 ? bem_init_t<double2>(ctx, n, ws, eps, nvec, k0) : bem_init_t<float2>(ctx, n, ws, eps, nvec, k0);
+  StageTimer tm;
+  if (phase_ms)
+    for (cudaEvent_t& e : tm.ev) BEM_CUDA_CHECK(cudaEventCreate(&e));
+  StageTimer* tp = phase_ms ? &tm : nullptr;
+  int st = precision == 0 ? bem_init_t<double2>(ctx, n, ws, eps, nvec, k0, tp)
+                          : bem_init_t<float2>(ctx, n, ws, eps, nvec, k0, tp);
   if (st) return st;
+  if (phase_ms) {
+    BEM_CUDA_CHECK(cudaEventSynchronize(tm.ev[4]));
+    for (int i = 0; i < 4; ++i) BEM_CUDA_CHECK(cudaEventElapsedTime(&phase_ms[i], tm.ev[i], tm.ev[i + 1]));
+  }
   if (info_host) {
     int* dinfo = precision == 0 ? state_view<double2>(n, ws).info : state_view<float2>(n, ws).info;
     BEM_CUDA_CHECK(cudaMemcpyAsync(info_host, dinfo, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
@@ -804,7 +832,7 @@ int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face
                     const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
                     int32_t* info_host, void* stream) {
   return bem200_bem_init_ex(precision, engine, n, ws, eps_per_face, eps1, eps2, nvec, k0, gemm_ws, gemm_ws_bytes, 0, 0,
-                            info_host, stream);
+                            nullptr, info_host, stream);
 }
 
 size_t bem200_bem_solve_workspace_size(int precision, int n, int npol) {

@@ -69,7 +69,23 @@ def case_step(a):
     for _ in range(a.warmup):
         one()
     ms = _timed(one, a.steps)
-    return {"case": "step", "faces": cp.n, "precision": a.precision, "ms_per_step": ms, "ir": bem.last_ir}
+    # one more step with the init's stage timer and events around assembly / init / solve
+    bem._phase_buf = (ctypes.c_float * 4)()
+    bem.clear()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    e[0].record()
+    bem.init(650.0)
+    e[1].record()
+    bem.solve_device(bt, npol)
+    e[2].record()
+    torch.cuda.synchronize()
+    bem._phase_buf = None
+    ph = bem.last_init_phases_ms
+    return {"case": "step", "faces": cp.n, "precision": a.precision, "ms_per_step": ms, "ir": bem.last_ir,
+            "phases_ms": {"assembly_init_total": e[0].elapsed_time(e[1]), "solve_ir": e[1].elapsed_time(e[2]),
+                          "lu_g1_g2_sigma1_sigma2": ph[0], "lu_delta": ph[1], "delta_inverse": ph[2],
+                          "sigma_lu_sigma": ph[3]}}
 
 
 def case_green(a):
