@@ -28,6 +28,7 @@ struct BemState {
   int32_t* map[4];   // rowmaps of LU(G1), LU(G2), LU(Delta), LU(Sigma)
   int32_t* ipiv[4];  // LAPACK swap sequences of the same factors
   int32_t* snap[2];  // look-ahead LU scratch (2 n row-map snapshots + grid-panel slots), one per chain
+  C* dinv[6];        // diagonal-block inverses (L, U) of LU(G1), LU(G2), LU(Sigma) for the blocked solves
   int* info;
   int* status;
 };
@@ -38,7 +39,8 @@ template <typename C>
 static size_t state_bytes(int n) {
   size_t mat = align256(sizeof(C) * (size_t)n * n);
   return kSlots * mat + 8 * align256(sizeof(int32_t) * n) +
-         2 * (align256(sizeof(int32_t) * 2 * (size_t)n) + kPanelGridScratch) + 256;
+         2 * (align256(sizeof(int32_t) * 2 * (size_t)n) + kPanelGridScratch) + 6 * align256(trsv_diag_inverse_bytes<C>(n)) +
+         256;
 }
 
 template <typename C>
@@ -58,6 +60,10 @@ static BemState<C> state_view(int n, void* ws) {
   for (int i = 0; i < 2; ++i) {  // snapshots, then the grid-panel candidate slots
     s.snap[i] = reinterpret_cast<int32_t*>(p);
     p += align256(sizeof(int32_t) * 2 * (size_t)n) + kPanelGridScratch;
+  }
+  for (int i = 0; i < 6; ++i) {
+    s.dinv[i] = reinterpret_cast<C*>(p);
+    p += align256(trsv_diag_inverse_bytes<C>(n));
   }
   s.info = reinterpret_cast<int*>(p);
   s.status = s.info + 1;
@@ -174,6 +180,10 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
   if ((st = getrf<C>(c2, n, s.M[1], n, s.map[1], s.ipiv[1], s.snap[1]))) return st;
   if ((st = solve_right<C>(c, n, n, s.M[0], n, s.map[0], s.M[2], n, s.M[5]))) return st;
   if ((st = solve_right<C>(c2, n, n, s.M[1], n, s.map[1], s.M[3], n, fork ? s.M[4] : s.M[5]))) return st;
+  if constexpr (sizeof(C) == 8) {  // complex64: diagonal-block inverses for the refinement sweeps' solves
+    if ((st = trsv_diag_inverse<C>(c, n, s.M[0], n, s.map[0], s.dinv[0], s.dinv[1]))) return st;
+    if ((st = trsv_diag_inverse<C>(c2, n, s.M[1], n, s.map[1], s.dinv[2], s.dinv[3]))) return st;
+  }
   if (fork) {
     BEM_CUDA_CHECK(cudaEventRecord(fj.join, fj.side));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(ctx.stream, fj.join, 0));
@@ -191,6 +201,9 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
   sigma_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(n, s.M[2], s.M[3], s.M[5], nvec, eps, k0 * k0, s.M[6]);
   BEM_LAUNCH_CHECK();
   if ((st = getrf<C>(c, n, s.M[6], n, s.map[3], s.ipiv[3], s.snap[0]))) return st;
+  if constexpr (sizeof(C) == 8) {
+    if ((st = trsv_diag_inverse<C>(c, n, s.M[6], n, s.map[3], s.dinv[4], s.dinv[5]))) return st;
+  }
   return mark(4);
 }
 
@@ -336,7 +349,10 @@ static int bem_solve_core(const LaContext& ctx0, int n, int p, void* ws, const C
   solve_rhs_sig_kernel<C><<<ceil_div(np, 256), 256, 0, st_>>>(n, p, Dm, X, nvec, eps, k0, rs);
   BEM_LAUNCH_CHECK();
   // sig2 = Sigma^-1 rs   (in place in rs)
-  if ((st = solve_left<C>(ctx, n, p, s.M[6], n, s.map[3], rs, p, lscr))) return st;
+  const bool di = sizeof(C) == 8;  // complex64 factors carry diagonal-block inverses
+  if ((st = solve_left<C>(ctx, n, p, s.M[6], n, s.map[3], rs, p, lscr, di ? s.dinv[4] : nullptr,
+                          di ? s.dinv[5] : nullptr)))
+    return st;
   // h2 = Delta^-1 (ik n L sig2 + Am)
   solve_rhs_h_kernel<C><<<ceil_div(3 * np, 256), 256, 0, st_>>>(n, p, rs, Am, nvec, eps, k0, X);
   BEM_LAUNCH_CHECK();
@@ -354,8 +370,12 @@ static int bem_solve_core(const LaContext& ctx0, int n, int p, void* ws, const C
   LaContext c2 = ctx;
   c2.stream = fj.side;
   void* lscr2 = reinterpret_cast<char*>(lscr) + align256(solve_left_scratch_bytes<C>(n, 4 * p));
-  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[0], n, s.map[0], W1, 4 * p, lscr))) return st;
-  if ((st = solve_left<C>(c2, n, 4 * p, s.M[1], n, s.map[1], W2, 4 * p, lscr2))) return st;
+  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[0], n, s.map[0], W1, 4 * p, lscr, di ? s.dinv[0] : nullptr,
+                          di ? s.dinv[1] : nullptr)))
+    return st;
+  if ((st = solve_left<C>(c2, n, 4 * p, s.M[1], n, s.map[1], W2, 4 * p, lscr2, di ? s.dinv[2] : nullptr,
+                          di ? s.dinv[3] : nullptr)))
+    return st;
   BEM_CUDA_CHECK(cudaEventRecord(fj.join, fj.side));
   BEM_CUDA_CHECK(cudaStreamWaitEvent(st_, fj.join, 0));
   return BEM200_OK;

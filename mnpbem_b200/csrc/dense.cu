@@ -1465,10 +1465,20 @@ __device__ __forceinline__ void trsv_load_tile(C* dst, const RowView<C>& T, int 
 // backward.  kUnit: unit diagonal.  kTrans: the operator is T^T.  The LU
 // factors give (kLower, kUnit) = (true, true) for L and (false, false) for U;
 // their transposes U^T and L^T give (true, false) and (false, true).
+// a 64 x 64 row-major block -> dst (64 x kTrsvPitch)
+template <typename C>
+__device__ __forceinline__ void trsv_load_plain(C* dst, const C* __restrict__ src) {
+  for (int idx = threadIdx.x; idx < kTrsvBS * kTrsvBS; idx += blockDim.x)
+    cp_async_elem<sizeof(C)>(dst + (idx >> 6) * kTrsvPitch + (idx & 63), src + idx);
+}
+
+// Dinv (optional): the inverses of the 64 x 64 diagonal blocks of the operator
+// (trsv_diag_inverse); the diagonal step is then a parallel 64 x 64 product
+// instead of a 64-step sweep.
 template <typename C, bool kLower, bool kUnit, bool kTrans>
 __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowView<C> T, C* __restrict__ X,
                                                           int* __restrict__ flags, int* __restrict__ ticket,
-                                                          int* __restrict__ status) {
+                                                          int* __restrict__ status, const C* __restrict__ Dinv) {
   extern __shared__ __align__(16) unsigned char trsv_smem[];
   C* tiles = reinterpret_cast<C*>(trsv_smem);        // 2 x 64 x kTrsvPitch
   C* xs = tiles + 2 * kTrsvBS * kTrsvPitch;           // 64 x 16: this block's x
@@ -1487,9 +1497,14 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
   const int r0 = I * kTrsvBS, rb = min(kTrsvBS, n - r0);
   const int nsrc = tk;  // blocks this one depends on: I of them (lower) or nblk - 1 - I (upper)
   auto src_block = [&](int s) { return kLower ? s : nblk - 1 - s; };
+  auto load_block = [&](C* dst, int J) {  // dependency tile J, or the diagonal block (J == I)
+    if (J == I && Dinv)
+      trsv_load_plain<C>(dst, Dinv + (long long)I * kTrsvBS * kTrsvBS);
+    else
+      trsv_load_tile<C, kTrans>(dst, T, r0, rb, J * kTrsvBS, min(kTrsvBS, n - J * kTrsvBS));
+  };
   {  // tile 0: the first dependency, or the diagonal block
-    const int J = nsrc > 0 ? src_block(0) : I;
-    trsv_load_tile<C, kTrans>(tiles, T, r0, rb, J * kTrsvBS, min(kTrsvBS, n - J * kTrsvBS));
+    load_block(tiles, nsrc > 0 ? src_block(0) : I);
     cp_async_commit();
   }
   for (int idx = tid; idx < kTrsvBS * nrhs; idx += 256) {
@@ -1504,9 +1519,7 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
     const int J = src_block(s);
     const int c0 = J * kTrsvBS, cb = min(kTrsvBS, n - c0);
     {  // prefetch tile s + 1 (the next dependency or the diagonal block)
-      const int Jn = (s + 1 < nsrc) ? src_block(s + 1) : I;
-      trsv_load_tile<C, kTrans>(tiles + ((s + 1) & 1) * kTrsvBS * kTrsvPitch, T, r0, rb, Jn * kTrsvBS,
-                                 min(kTrsvBS, n - Jn * kTrsvBS));
+      load_block(tiles + ((s + 1) & 1) * kTrsvBS * kTrsvPitch, (s + 1 < nsrc) ? src_block(s + 1) : I);
       cp_async_commit();
     }
     if (tid == 0) {
@@ -1556,7 +1569,39 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
   }
   cp_async_wait<0>();
   __syncthreads();
-  if (!sabort) {
+  if (!sabort && Dinv) {
+    // x_I = Dinv_I x_I: the same split dot products as the dependency updates
+    const C* D = tiles + (nsrc & 1) * kTrsvBS * kTrsvPitch;
+    for (int idx = tid; idx < kTrsvBS * nrhs; idx += 256) {
+      const int r = idx / nrhs, q = idx % nrhs;
+      xj[r * kTrsvMaxRhs + q] = xs[r * kTrsvMaxRhs + q];
+    }
+    __syncthreads();
+    for (int base = 0; base < nout * S; base += 256) {
+      const int idx = base + tid;
+      const int o = idx / S, part = idx % S;
+      C acc = czero<C>();
+      if (o < nout) {
+        const int r = o / nrhs, q = o % nrhs;
+        const C* drow = D + r * kTrsvPitch;
+#pragma unroll 8
+        for (int c = part; c < kTrsvBS; c += S) acc = cadd(acc, cmul(drow[c], xj[c * kTrsvMaxRhs + q]));
+      }
+      for (int off = 1; off < S; off <<= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+      }
+      if (o < nout && part == 0) {
+        const int r = o / nrhs, q = o % nrhs;
+        xs[r * kTrsvMaxRhs + q] = acc;
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < rb * nrhs; idx += 256) {
+      const int r = idx / nrhs, q = idx % nrhs;
+      X[(long long)(r0 + r) * nrhs + q] = xs[r * kTrsvMaxRhs + q];
+    }
+  } else if (!sabort) {
     const C* D = tiles + (nsrc & 1) * kTrsvBS * kTrsvPitch;  // the diagonal block
     for (int q = wid; q < nrhs; q += 8) {
       C x0 = xs[lane * kTrsvMaxRhs + q], x1 = xs[(lane + 32) * kTrsvMaxRhs + q];
@@ -1608,13 +1653,72 @@ __global__ void __launch_bounds__(256) trsv_blocked_kernel(int n, int nrhs, RowV
   if (tid == 0) atomicExch(&flags[I], 1);
 }
 
+// Inverses of the 64 x 64 diagonal blocks of the factor (LU, rowmap): DL[I] =
+// L_II^-1 (unit lower), DU[I] = U_II^-1 (upper), each 64 x 64 row-major, rows
+// beyond n padded with the identity.  One CTA of 64 threads per block; thread
+// c computes column c of each inverse by substitution.  Used by the blocked
+// triangular solve so that the diagonal step of every block is a parallel
+// product (the factors are reused for several solves per factorisation).
+template <typename C>
+__global__ void __launch_bounds__(64) trsv_diag_inverse_kernel(int n, RowView<C> T, C* __restrict__ DL,
+                                                              C* __restrict__ DU) {
+  extern __shared__ __align__(16) unsigned char dinv_smem[];
+  C(*blk)[kTrsvBS + 1] = reinterpret_cast<C(*)[kTrsvBS + 1]>(dinv_smem);
+  C(*X)[kTrsvBS + 1] = blk + kTrsvBS;
+  const int I = blockIdx.x, r0 = I * kTrsvBS, rb = min(kTrsvBS, n - r0);
+  const int c = threadIdx.x;
+  const C one = cmake<C>(1.0, 0.0), zero = czero<C>();
+  for (int r = 0; r < kTrsvBS; ++r)
+    blk[r][c] = (r < rb && c < rb) ? T.at(r0 + r, r0 + c) : (r == c ? one : zero);
+  __syncthreads();
+  // L^-1: x_r = 0 (r < c), x_c = 1, x_r = -sum_{c <= k < r} L_rk x_k (r > c)
+  for (int r = 0; r < kTrsvBS; ++r) {
+    C x = (r == c) ? one : zero;
+    if (r > c)
+      for (int k = c; k < r; ++k) x = csub(x, cmul(blk[r][k], X[k][c]));
+    X[r][c] = x;
+  }
+  C* dl = DL + (long long)I * kTrsvBS * kTrsvBS;
+  for (int r = 0; r < kTrsvBS; ++r) dl[r * kTrsvBS + c] = X[r][c];
+  // U^-1: x_r = 0 (r > c), x_c = 1 / U_cc, x_r = -(sum_{r < k <= c} U_rk x_k) / U_rr (r < c, descending)
+  for (int r = kTrsvBS - 1; r >= 0; --r) {
+    C x = zero;
+    if (r <= c) {
+      C acc = (r == c) ? one : zero;
+      for (int k = r + 1; k <= c; ++k) acc = csub(acc, cmul(blk[r][k], X[k][c]));
+      const C d = blk[r][r];
+      x = cabs1(d) > 0 ? cdiv(acc, d) : zero;
+    }
+    X[r][c] = x;
+  }
+  C* du = DU + (long long)I * kTrsvBS * kTrsvBS;
+  for (int r = 0; r < kTrsvBS; ++r) du[r * kTrsvBS + c] = X[r][c];
+}
+
+template <typename C>
+size_t trsv_diag_inverse_bytes(int n) {
+  return sizeof(C) * (size_t)ceil_div(n, kTrsvBS) * kTrsvBS * kTrsvBS;
+}
+
+template <typename C>
+int trsv_diag_inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_t* rowmap, C* DL, C* DU) {
+  RowView<C> T{const_cast<C*>(LU), ld, rowmap, 0};
+  const size_t smem = sizeof(C) * 2 * kTrsvBS * (kTrsvBS + 1);
+  int st = prep_smem(trsv_diag_inverse_kernel<C>, smem);
+  if (st) return st;
+  trsv_diag_inverse_kernel<C><<<ceil_div(n, kTrsvBS), kTrsvBS, smem, ctx.stream>>>(n, T, DL, DU);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
 template <typename C>
 static size_t trsv_smem_bytes() {
   return sizeof(C) * (2 * kTrsvBS * kTrsvPitch + 2 * kTrsvBS * kTrsvMaxRhs);
 }
 
 template <typename C, bool kLower, bool kUnit = kLower, bool kTrans = false>
-static int trsv_blocked(const LaContext& ctx, int n, int nrhs, RowView<C> T, C* X, int* iscratch) {
+static int trsv_blocked(const LaContext& ctx, int n, int nrhs, RowView<C> T, C* X, int* iscratch,
+                        const C* Dinv = nullptr) {
   const int nblk = ceil_div(n, kTrsvBS);
   // iscratch: flags [0, nblk), ticket [nblk], local status [nblk + 1]
   BEM_CUDA_CHECK(cudaMemsetAsync(iscratch, 0, sizeof(int) * (nblk + 2), ctx.stream));
@@ -1622,7 +1726,7 @@ static int trsv_blocked(const LaContext& ctx, int n, int nrhs, RowView<C> T, C* 
   int st = prep_smem(kern, trsv_smem_bytes<C>());
   if (st) return st;
   kern<<<nblk, 256, trsv_smem_bytes<C>(), ctx.stream>>>(n, nrhs, T, X, iscratch, iscratch + nblk,
-                                                        ctx.dstatus ? ctx.dstatus : iscratch + nblk + 1);
+                                                        ctx.dstatus ? ctx.dstatus : iscratch + nblk + 1, Dinv);
   BEM_LAUNCH_CHECK();
   return BEM200_OK;
 }
@@ -1783,7 +1887,7 @@ size_t solve_left_scratch_bytes(int n, int nrhs) {
 
 template <typename C>
 int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld, const int32_t* rowmap, C* B,
-               long long ldb, void* scratch) {
+               long long ldb, void* scratch, const C* dinv_l, const C* dinv_u) {
   if (nrhs <= 0) return BEM200_OK;
   BEM_REQUIRE(scratch, BEM200_ERR_ARG, "solve_left: scratch required");
   C* Y = reinterpret_cast<C*>(scratch);
@@ -1794,8 +1898,8 @@ int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld,
   RowView<C> T{const_cast<C*>(LU), ld, rowmap, 0};
   int st;
   if (nrhs <= kTrsvMaxRhs) {
-    if ((st = trsv_blocked<C, true>(ctx, n, nrhs, T, Y, iscr))) return st;
-    if ((st = trsv_blocked<C, false>(ctx, n, nrhs, T, Y, iscr))) return st;
+    if ((st = trsv_blocked<C, true>(ctx, n, nrhs, T, Y, iscr, dinv_l))) return st;
+    if ((st = trsv_blocked<C, false>(ctx, n, nrhs, T, Y, iscr, dinv_u))) return st;
   } else {
     if ((st = trsm_llu<C>(ctx, n, nrhs, T, plain(Y, nrhs)))) return st;
     if ((st = trsm_lun<C>(ctx, n, nrhs, T, plain(Y, nrhs)))) return st;
@@ -2010,7 +2114,9 @@ int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_
   template int getrf<C>(const LaContext&, int, C*, long long, int32_t*, int32_t*, int32_t*);                     \
   template size_t solve_left_scratch_bytes<C>(int, int);                                                         \
   template int solve_left<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long,     \
-                             void*);                                                                             \
+                             void*, const C*, const C*);                                                         \
+  template size_t trsv_diag_inverse_bytes<C>(int);                                                               \
+  template int trsv_diag_inverse<C>(const LaContext&, int, const C*, long long, const int32_t*, C*, C*);         \
   template int solve_right<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long, C*); \
   template int inverse<C>(const LaContext&, int, const C*, long long, const int32_t*, C*, long long);         \
   template int solve_left_T<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long,   \

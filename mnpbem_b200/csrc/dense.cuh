@@ -125,9 +125,18 @@ int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int3
 // solve_left_scratch_bytes.
 template <typename C>
 size_t solve_left_scratch_bytes(int n, int nrhs);
+// dinv_l / dinv_u (optional): the diagonal-block inverses of trsv_diag_inverse.
 template <typename C>
 int solve_left(const LaContext& ctx, int n, int nrhs, const C* LU, long long ld, const int32_t* rowmap, C* B,
-               long long ldb, void* scratch);
+               long long ldb, void* scratch, const C* dinv_l = nullptr, const C* dinv_u = nullptr);
+
+// Inverses of the 64 x 64 diagonal blocks of L and U of a factor, for the
+// blocked triangular solves of solve_left: DL, DU trsv_diag_inverse_bytes(n)
+// each.
+template <typename C>
+size_t trsv_diag_inverse_bytes(int n);
+template <typename C>
+int trsv_diag_inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_t* rowmap, C* DL, C* DU);
 
 // B <- A^-T B for the factor (LU, rowmap) (transposed solve, nrhs <= 16);
 // scratch: solve_left_scratch_bytes.
