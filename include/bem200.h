@@ -201,18 +201,20 @@ size_t bem200_gemm_workspace_size(int engine, int m, int n, int k);
  * U) is storage row rowmap[i].  ipiv[k] = logical row exchanged with row k
  * (LAPACK swap sequence, 0-based); *info = first exactly-zero pivot (1-based)
  * or 0.  All arrays are device.
- * complex128: partial pivoting (largest |re|+|im|), LAPACK's pivots.
- * complex64: panels of more than 512 rows choose their 32 pivot rows by
- * tournament pivoting (each CTA of a cluster nominates the pivots of its own
- * rows, one CTA factors the nominees; Grigori, Demmel & Xiang, SIAM J.
- * Matrix Anal. Appl. 32, 2011): one cluster-wide exchange per panel instead
- * of one per column, pivots that may differ from LAPACK's.  Shorter panels
- * use partial pivoting.  Replaces the LU factorisations of BEMRet.init
- * (mnpbem/bem/bem_ret.py:437-523, via mnpbem/utils/gpu.py:145).
- * bem200_getrf_ex: flags BEM200_GETRF_PARTIAL_PIVOTING = partial pivoting
- * for complex64 too; lookahead_nb = block width of the look-ahead schedule
- * (multiple of 32 in [64, 1024]; 0 = 128). */
+ * Partial pivoting (largest |re|+|im|), LAPACK's pivots, for both dtypes.
+ * Replaces the LU factorisations of BEMRet.init (mnpbem/bem/bem_ret.py:437-523,
+ * via mnpbem/utils/gpu.py:145).
+ * bem200_getrf_ex: flags BEM200_GETRF_TOURNAMENT_PIVOTING = complex64 panels
+ * of more than 512 rows choose their 32 pivot rows by tournament pivoting
+ * (each CTA of a cluster nominates the pivots of its own rows, one CTA
+ * factors the nominees; Grigori, Demmel & Xiang, SIAM J. Matrix Anal. Appl.
+ * 32, 2011): one cluster-wide exchange per panel instead of one per column,
+ * pivots that may differ from LAPACK's (measured slower than partial
+ * pivoting at n = 5768 on B200, so off by default).  BEM200_GETRF_PARTIAL_
+ * PIVOTING (the default) is accepted and wins over it.  lookahead_nb = block
+ * width of the look-ahead schedule (multiple of 32 in [64, 1024]; 0 = 128). */
 #define BEM200_GETRF_PARTIAL_PIVOTING 1
+#define BEM200_GETRF_TOURNAMENT_PIVOTING 2
 int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
                  int32_t* info, void* ws, size_t ws_bytes, void* stream);
 int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
@@ -271,8 +273,8 @@ int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face
                     const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
                     int32_t* info_host, void* stream);
 /* bem200_bem_init with the LU tiling exposed (for the project's autotuner):
- * lu_flags BEM200_GETRF_PARTIAL_PIVOTING (complex64 factors with partial
- * pivoting instead of tournament panels), lookahead_nb the block width of the
+ * lu_flags as bem200_getrf_ex's (BEM200_GETRF_TOURNAMENT_PIVOTING: complex64
+ * factors with tournament panels), lookahead_nb the block width of the
  * look-ahead LU schedule (a multiple of 32 in [64, 1024]; 0 = 128).
  * phase_ms (HOST, 4 floats, or NULL): stage timer (CUDA events on the
  * stream; the call then synchronises): LU(G1) || LU(G2) with Sigma1 || Sigma2,

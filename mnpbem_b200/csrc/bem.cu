@@ -818,14 +818,14 @@ int bem200_bem_init_ex(int precision, int engine, int n, void* ws, int eps_per_f
                        const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
                        int lu_flags, int lookahead_nb, float* phase_ms, int32_t* info_host, void* stream) {
   BEM_REQUIRE(n > 0 && ws && eps1 && eps2 && nvec, BEM200_ERR_ARG, "bem_init: bad arguments");
-  BEM_REQUIRE((lu_flags & ~BEM200_GETRF_PARTIAL_PIVOTING) == 0, BEM200_ERR_ARG, "bem_init: unknown LU flags 0x%x",
+  BEM_REQUIRE((lu_flags & ~(BEM200_GETRF_PARTIAL_PIVOTING | BEM200_GETRF_TOURNAMENT_PIVOTING)) == 0, BEM200_ERR_ARG, "bem_init: unknown LU flags 0x%x",
               lu_flags);
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
   ctx.engine = engine_from(engine);
   ctx.ws = gemm_ws;
   ctx.ws_bytes = gemm_ws_bytes;
-  ctx.tournament = (lu_flags & BEM200_GETRF_PARTIAL_PIVOTING) == 0;
+  ctx.tournament = (lu_flags & BEM200_GETRF_TOURNAMENT_PIVOTING) && !(lu_flags & BEM200_GETRF_PARTIAL_PIVOTING);
   ctx.la_nb = lookahead_nb;
   EpsArg eps = make_eps(eps_per_face, eps1, eps2);
   StageTimer tm;

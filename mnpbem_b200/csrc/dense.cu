@@ -2173,14 +2173,14 @@ size_t bem200_getrf_workspace_size(int dtype, int engine, int n) {
 
 int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv, int32_t* info,
                     void* ws, size_t ws_bytes, int flags, int lookahead_nb, void* stream) {
-  BEM_REQUIRE((flags & ~BEM200_GETRF_PARTIAL_PIVOTING) == 0, BEM200_ERR_ARG, "getrf: unknown flags 0x%x", flags);
+  BEM_REQUIRE((flags & ~(BEM200_GETRF_PARTIAL_PIVOTING | BEM200_GETRF_TOURNAMENT_PIVOTING)) == 0, BEM200_ERR_ARG, "getrf: unknown flags 0x%x", flags);
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
   ctx.engine = engine_of(engine);
   ctx.ws = ws;
   ctx.ws_bytes = ws_bytes;
   ctx.dinfo = info;
-  ctx.tournament = (flags & BEM200_GETRF_PARTIAL_PIVOTING) == 0;
+  ctx.tournament = (flags & BEM200_GETRF_TOURNAMENT_PIVOTING) && !(flags & BEM200_GETRF_PARTIAL_PIVOTING);
   ctx.la_nb = lookahead_nb;
   int32_t* snap = nullptr;
   if (ws && n > 0 && ws_bytes >= bem200_getrf_workspace_size(dtype, engine, n)) {

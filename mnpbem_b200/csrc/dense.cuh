@@ -59,7 +59,7 @@ struct LaContext {
   int* dinfo = nullptr;     // device int: first exactly-zero pivot (1-based) or 0
   int* dstatus = nullptr;   // device int: set to a non-zero code if a bounded wait gave up
   void* panel_ws = nullptr; // candidate slots of the grid-wide panel (panels of more rows than a cluster holds)
-  bool tournament = true;   // complex64 panels: tournament pivoting (false: partial pivoting, LAPACK's pivots)
+  bool tournament = false;  // complex64 panels: tournament pivoting (false: partial pivoting, LAPACK's pivots)
   int la_nb = 0;            // look-ahead block width of getrf (multiple of 32; 0 = 128)
 };
 

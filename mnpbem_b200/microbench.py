@@ -3,7 +3,7 @@
     python -m mnpbem_b200.microbench step  [--faces 1444] [--precision mixed|fp64] [--steps 1] [--warmup 1]
     python -m mnpbem_b200.microbench green [--faces 1444] [--dtype c128|c64] [--reps 3]
     python -m mnpbem_b200.microbench gemm  [--m 5768 --n 2884 --k 2884] [--engine 1] [--reps 3]
-    python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1] [--partial]
+    python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1] [--tournament]
     python -m mnpbem_b200.microbench hmat  [--faces 1444] [--cleaf 200] [--htol 1e-6] [--reps 3]
     python -m mnpbem_b200.microbench iter  [--faces 1444] [--hmatrix] [--noprecond] [--tol 1e-10]
     python -m mnpbem_b200.microbench large [--side 3 | --shape cube] [--hmatrix] [--tol 1e-8]
@@ -140,7 +140,7 @@ def case_getrf(a):
     wsb = int(nat.lib().bem200_getrf_workspace_size(code, a.engine, n))
     ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
 
-    flags = 1 if a.partial else 0
+    flags = 2 if a.tournament else 0
 
     def go():
         A.copy_(A0)
@@ -167,7 +167,7 @@ def case_getrf(a):
     else:
         ms = _timed(go, a.reps)
     return {"case": "getrf", "n": n, "dtype": a.dtype, "engine": a.engine, "graph": bool(a.graph),
-            "pivoting": "partial" if a.partial else "tournament (complex64 panels > 512 rows)", "ms": ms,
+            "pivoting": "tournament (complex64 panels > 512 rows)" if a.tournament else "partial", "ms": ms,
             "TFLOPs": 8.0 / 3.0 * n ** 3 / ms / 1e9, "info": int(info.item()), "backward_error": berr}
 
 
@@ -467,7 +467,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--graph", action="store_true", help="getrf: replay from a CUDA graph")
-    ap.add_argument("--partial", action="store_true", help="getrf: partial pivoting for complex64 too")
+    ap.add_argument("--tournament", action="store_true", help="getrf: tournament pivoting of complex64 panels")
     ap.add_argument("--la-nb", dest="la_nb", type=int, default=0, help="getrf: look-ahead block width (0 = 128)")
     ap.add_argument("--cleaf", type=int, default=200)
     ap.add_argument("--htol", type=float, default=1e-6)

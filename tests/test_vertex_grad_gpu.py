@@ -106,7 +106,7 @@ def test_vertex_gradient_matches_reference_fd(cuda, precision):
     assert err < 1e-6, (dext, g["dext"], err)
 
 
-def _fd(cp, D, enei, pol, dirs, h=1e-4):
+def _fd(cp, D, enei, pol, dirs, h=1e-3):
     from mnpbem_b200 import BEMRet, PlaneWaveRet
     from mnpbem_b200.shape import perturbed
     exc = PlaneWaveRet(pol, dirs)
@@ -128,7 +128,9 @@ def test_vertex_gradient_matches_solver_fd(cuda, mk, enei):
     bem = _bem(cp, enei, "fp64")
     wts = np.array([1.0, 0.5])
     ext, grad = extinction_vertex_vjp(bem, PlaneWaveRet(pol, dirs), enei, weights=wts)
+    # central differences with h = 1e-3 nm: truncation (h / radius)^2 ~ 1e-8,
+    # the FP64 solves' own noise (~1e-12 of ext) / 2h ~ 1e-7 of the slope
     for D in random_directions(cp, 2, seed=7):
         ref = float(np.dot(wts, _fd(cp, D, enei, pol, dirs)))
         got = float(np.sum(grad * D))
-        assert abs(got - ref) <= 1e-6 * max(abs(ref), 1e-3 * np.max(np.abs(ext))), (got, ref)
+        assert abs(got - ref) <= 2e-6 * max(abs(ref), 1e-3 * np.max(np.abs(ext))), (got, ref)
