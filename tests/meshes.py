@@ -1,4 +1,6 @@
 """Seeded test meshes shared by the CPU and GPU tests."""
+import contextlib
+
 import numpy as np
 
 from mnpbem_b200.geometry import ComParticle, trisphere
@@ -62,3 +64,29 @@ def face_nodes(p):
     ok = ~np.isnan(f)
     out[:, :f.shape[1]][ok] = v[f[ok].astype(int)]
     return out
+
+
+@contextlib.contextmanager
+def refinement_of(base):
+    """Meshes solved inside this context refine exactly the face pairs that
+    `base` refines (the selection of bem200_refine_count / _fill is made from
+    base's centroids and boundary radii).  The reverse-mode gradient holds the
+    refinement pattern fixed, so central differences of perturbed meshes must
+    too: on fine meshes some pair distances cross the cutoff within a step of
+    1e-3 nm, and the quadrature switch of such a pair is a jump in ext."""
+    import torch
+    from mnpbem_b200 import _native as nat
+    f64 = dict(dtype=torch.float64, device="cuda")
+    pos0 = torch.as_tensor(np.ascontiguousarray(base.pos), **f64)
+    rad0 = torch.as_tensor(np.ascontiguousarray(base.bradius()), **f64)
+    real = nat.call
+
+    def call(name, *args):
+        if name in ("bem200_refine_count", "bem200_refine_fill"):
+            args = (args[0], nat.ptr(pos0), nat.ptr(rad0)) + tuple(args[3:])
+        return real(name, *args)
+    nat.call = call
+    try:
+        yield
+    finally:
+        nat.call = real

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from conftest import golden
-from meshes import dimer, shape_particle, sphere
+from meshes import dimer, refinement_of, shape_particle, sphere
 
 pytestmark = pytest.mark.gpu
 
@@ -111,9 +111,10 @@ def _fd(cp, D, enei, pol, dirs, h=1e-3):
     from mnpbem_b200.shape import perturbed
     exc = PlaneWaveRet(pol, dirs)
     out = []
-    for s in (1.0, -1.0):
-        q = perturbed(cp, s * h * D)
-        out.append(BEMRet(q).cross_sections(exc, enei)["ext"])
+    with refinement_of(cp):
+        for s in (1.0, -1.0):
+            q = perturbed(cp, s * h * D)
+            out.append(BEMRet(q).cross_sections(exc, enei)["ext"])
     return (out[0] - out[1]) / (2 * h)
 
 
@@ -128,8 +129,11 @@ def test_vertex_gradient_matches_solver_fd(cuda, mk, enei):
     bem = _bem(cp, enei, "fp64")
     wts = np.array([1.0, 0.5])
     ext, grad = extinction_vertex_vjp(bem, PlaneWaveRet(pol, dirs), enei, weights=wts)
-    # central differences with h = 1e-3 nm: truncation (h / radius)^2 ~ 1e-8,
-    # the FP64 solves' own noise (~1e-12 of ext) / 2h ~ 1e-7 of the slope
+    # ext is invariant under translation of the whole mesh
+    assert np.all(np.abs(grad.sum(axis=0)) <= 1e-9 * np.abs(grad).sum(axis=0)), grad.sum(axis=0)
+    # central differences with h = 1e-3 nm and the unperturbed refinement
+    # pattern: truncation (h / radius)^2 ~ 1e-8, the FP64 solves' own noise
+    # (~1e-12 of ext) / 2h ~ 1e-7 of the slope
     for D in random_directions(cp, 2, seed=7):
         ref = float(np.dot(wts, _fd(cp, D, enei, pol, dirs)))
         got = float(np.sum(grad * D))
