@@ -201,7 +201,11 @@ size_t bem200_gemm_workspace_size(int engine, int m, int n, int k);
  * U) is storage row rowmap[i].  ipiv[k] = logical row exchanged with row k
  * (LAPACK swap sequence, 0-based); *info = first exactly-zero pivot (1-based)
  * or 0.  All arrays are device.
- * Partial pivoting (largest |re|+|im|), LAPACK's pivots, for both dtypes.
+ * Partial pivoting (largest |re|+|im|, first maximum on ties), LAPACK's
+ * pivots, for both dtypes.  complex64 multipliers use an approximate
+ * reciprocal of |pivot|^2 (last-bit differences from cgetrf's division).
+ * *info = -BEM200_ERR_TIMEOUT if a bounded device-side wait of a complex64
+ * panel gave up (the factors are then invalid).
  * Replaces the LU factorisations of BEMRet.init (mnpbem/bem/bem_ret.py:437-523,
  * via mnpbem/utils/gpu.py:145).
  * bem200_getrf_ex: flags BEM200_GETRF_TOURNAMENT_PIVOTING = complex64 panels

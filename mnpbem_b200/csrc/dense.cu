@@ -752,6 +752,274 @@ __global__ void __launch_bounds__(kPushThreads, 1) panel_lu_push_kernel(int m, i
 }
 
 // ----------------------------------------------------------------------------
+// Asynchronous push panel (complex64): the push panel's layout (one panel row
+// per thread, in registers) with the cluster barrier of every column replaced
+// by one-way DSMEM messages, and the rank-1 update of the remaining columns
+// moved off the pivot search's critical path.
+//  * Exchange: the warp holding the CTA's best row sends it (32 elements and
+//    a 16-byte header: key, row, multiplier) to slot t % 3 of every CTA with
+//    st.async, which signals the receiver's mbarrier (complete_tx).  Each CTA
+//    arms its own barrier for cs * 272 bytes and waits for it; nobody waits
+//    for an acknowledgement.  A CTA sends column t + 1 only after it received
+//    all of column t, so a slot is rewritten only after every CTA has read it.
+//  * Deferred update: after sending column t's candidate, a thread applies
+//    pivot t - 1 to its columns > t while the candidates travel.  The column
+//    that decides the next pivot (t + 1) is updated right after the pivot is
+//    known.  Sent rows therefore lack pivot t - 1 in their columns > t; the
+//    header carries their multiplier l, and every CTA rebuilds the pivot row
+//    F = P - l F_prev (warp 0, one element per lane) for the next update.
+//  * Keys: 1 + the bit pattern of |re| + |im| (monotonic for non-negative
+//    floats; 0 = no candidate), reduced with redux.sync; equal keys go to the
+//    lowest row, as LAPACK's first maximum.
+//  * Multipliers use an approximate reciprocal of |pivot|^2 (rcp.approx);
+//    the factors are preconditioners of the refinement, so they differ from
+//    the exact-division ones in the last bits only.
+// Every mbarrier wait is bounded; on timeout the CTA records it, finishes
+// its loop without waiting and the status (or *info = -BEM200_ERR_TIMEOUT)
+// reports it.  A final cluster barrier keeps every CTA alive until all have
+// sent their last messages.
+constexpr int kAsyncThreads = 384;
+constexpr int kAsyncWarps = kAsyncThreads / 32;
+constexpr int kAsyncMaxCluster = 16;
+constexpr int kAsyncSpin = 1 << 22;
+
+struct __align__(16) AsyncHdr {
+  unsigned key;
+  int row;
+  float lx, ly;
+};
+
+struct AsyncShared {
+  float2 cand[3][kAsyncMaxCluster][kPanelNB];  // received candidate rows, by slot and sender
+  AsyncHdr hdr[3][kAsyncMaxCluster];
+  uint64_t bar[3];
+  float2 F[2][kPanelNB];  // pivot rows with the previous pivot applied
+  float2 Q[2][kPanelNB];  // (-F.y, F.x), for the packed update
+  float2 park[kPanelNB];  // the CTA winner's row, staged for its warp
+  unsigned wkey[2][kAsyncWarps];
+  int wrow[2][kAsyncWarps];
+  float2 wl[2][kAsyncWarps];
+  int perm[kPanelNB];
+  int singular;
+  int timeout;
+};
+
+__device__ __forceinline__ uint32_t as_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint32_t dsmem_map(uint32_t a, int rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_async_f2(uint32_t ra, float2 v, uint32_t rbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(ra),
+               "f"(v.x), "f"(v.y), "r"(rbar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async_v4(uint32_t ra, uint32_t a, uint32_t b, uint32_t c, uint32_t d,
+                                            uint32_t rbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(
+                   ra),
+               "r"(a), "r"(b), "r"(c), "r"(d), "r"(rbar)
+               : "memory");
+}
+__device__ __forceinline__ void async_bar_init(uint64_t* b) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(as_smem(b)));
+}
+__device__ __forceinline__ void async_bar_arm(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(as_smem(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool async_bar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(as_smem(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned redux_max_u32(unsigned v) {
+  unsigned r;
+  asm volatile("redux.sync.max.u32 %0, %1, 0xffffffff;" : "=r"(r) : "r"(v));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_bits(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 bits_f2(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+// c - a * b as two packed FMAs (fma.rn.f32x2); q = (-b.y, b.x)
+__device__ __forceinline__ float2 cfms_packed(float2 c, float2 a, float2 b, float2 q) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(make_float2(-a.x, -a.x))), "l"(f2_bits(b)),
+      "l"(f2_bits(c)));
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(make_float2(-a.y, -a.y))), "l"(f2_bits(q)), "l"(d));
+  return bits_f2(d);
+}
+__device__ __forceinline__ float2 crecip_approx(float2 p) {
+  const float d = p.x * p.x + p.y * p.y;
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  return d > 0.f ? make_float2(p.x * r, -p.y * r) : make_float2(0.f, 0.f);
+}
+__device__ __forceinline__ unsigned async_key(bool act, float2 a) { return act ? 1u + __float_as_uint(pmag(a)) : 0u; }
+
+__global__ void __launch_bounds__(kAsyncThreads, 1)
+    panel_lu_async_kernel(int m, int w, float2* __restrict__ A, long long ld, int col, int32_t* __restrict__ rowmap,
+                          int32_t* __restrict__ ipiv, int ipiv_base, int* __restrict__ info,
+                          int* __restrict__ status, int R) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int cs = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  __shared__ AsyncShared sh;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nwarps = (int)(blockDim.x >> 5);
+  const int r0 = rank * R;
+  const int rcount = max(0, min(R, m - r0));
+  const int prow_id = r0 + tid;
+  bool act = tid < rcount;
+  float2* arow = A + (act ? (long long)rowmap[prow_id] * ld : 0) + col;
+  float2 v[kPanelNB];
+#pragma unroll
+  for (int c = 0; c < kPanelNB; ++c) v[c] = (act && c < w) ? arow[c] : czero<float2>();
+  if (tid == 0) {
+    sh.singular = 0;
+    sh.timeout = 0;
+    for (int i = 0; i < 3; ++i) async_bar_init(&sh.bar[i]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (tid < kPanelNB) sh.F[1][tid] = sh.Q[1][tid] = czero<float2>();
+  float2 cur = v[0], lprev = czero<float2>(), ucur = czero<float2>();
+  int td = -1;
+  bool timed_out = false;
+  const uint32_t bytes = (uint32_t)cs * (uint32_t)(kPanelNB * sizeof(float2) + sizeof(AsyncHdr));
+  cluster.sync();  // barriers initialised in every CTA before the first message
+
+#pragma unroll 1
+  for (int t = 0; t < w; ++t) {
+    const int s = t % 3, b = t & 1;
+    if (tid == 0) async_bar_arm(&sh.bar[s], bytes);
+    // warp candidate
+    const unsigned key = async_key(act, cur);
+    const unsigned wk = redux_max_u32(key);
+    const int wl = __ffs(__ballot_sync(0xffffffffu, key == wk)) - 1;
+    if (lane == wl) sh.wl[b][wid] = lprev;
+    if (lane == 0) {
+      sh.wkey[b][wid] = wk;
+      sh.wrow[b][wid] = wk ? r0 + wid * 32 + wl : INT_MAX;
+    }
+    __syncthreads();
+    // CTA candidate: its warp stages the row and sends it to every CTA
+    const unsigned k2 = lane < nwarps ? sh.wkey[b][lane] : 0u;
+    const unsigned ck = redux_max_u32(k2);
+    const int ww = __ffs(__ballot_sync(0xffffffffu, lane < nwarps && k2 == ck)) - 1;
+    if (wid == ww) {
+      if (lane == wl && key != 0) {
+#pragma unroll
+        for (int c = 0; c < kPanelNB; ++c) sh.park[c] = v[c];
+        sh.park[t] = cur;
+      }
+      __syncwarp();
+      const float2 e = sh.park[lane];
+      const float2 lw = sh.wl[b][ww];
+      const uint32_t la = as_smem(&sh.cand[s][rank][lane]), lh = as_smem(&sh.hdr[s][rank]),
+                     lb = as_smem(&sh.bar[s]);
+      for (int d = 0; d < cs; ++d) {
+        const uint32_t rb = dsmem_map(lb, d);
+        st_async_f2(dsmem_map(la, d), e, rb);
+        if (lane == 0)
+          st_async_v4(dsmem_map(lh, d), ck, (uint32_t)sh.wrow[b][ww], __float_as_uint(lw.x), __float_as_uint(lw.y),
+                      rb);
+      }
+    }
+    // while the candidates travel: pivot t - 1 on this row's columns > t
+    if (act && t > 0) {
+      const float2* F = sh.F[b ^ 1];
+      const float2* Q = sh.Q[b ^ 1];
+#pragma unroll
+      for (int g = 0; g < kPanelNB; g += 8) {
+        if (g + 7 > t) {
+#pragma unroll
+          for (int c = g; c < g + 8; ++c)
+            if (c > t) v[c] = cfms_packed(v[c], lprev, F[c], Q[c]);
+        }
+      }
+    }
+    float2 nxt = v[0];
+#pragma unroll
+    for (int c = 1; c < kPanelNB; ++c)
+      if (c == t + 1) nxt = v[c];
+    // every CTA's candidate for column t has arrived
+    if (!timed_out) {
+      bool ok = false;
+      for (int it = 0; it < kAsyncSpin; ++it) {
+        if (async_bar_try(&sh.bar[s], (uint32_t)(t / 3) & 1u)) {
+          ok = true;
+          break;
+        }
+        if (it > 64) __nanosleep(32);
+      }
+      if (!ok) {
+        timed_out = true;
+        sh.timeout = 1;
+      }
+    }
+    const unsigned k3 = lane < cs ? sh.hdr[s][lane].key : 0u;
+    const unsigned gk = redux_max_u32(k3);
+    const int wc = __ffs(__ballot_sync(0xffffffffu, lane < cs && k3 == gk)) - 1;
+    const AsyncHdr h = sh.hdr[s][wc];
+    const int p = min(max(h.row, 0), m - 1);
+    const float2* P = sh.cand[s][wc];
+    const float2* Fp = sh.F[b ^ 1];
+    const float2 lw = t > 0 ? make_float2(h.lx, h.ly) : czero<float2>();
+    if (tid == 0) {
+      sh.perm[t] = p;
+      if (gk <= 1u && !sh.singular) sh.singular = t + 1;
+    }
+    if (wid == 0) {  // the pivot row with pivot t - 1 applied, for the next column's update
+      float2 f = P[lane];
+      if (lane > t) f = csub(f, cmul(lw, Fp[lane]));
+      sh.F[b][lane] = f;
+      sh.Q[b][lane] = make_float2(-f.y, f.x);
+    }
+    const float2 inv = crecip_approx(P[t]);
+    if (act) {
+      if (prow_id == p) {  // the pivot row becomes a row of U
+        act = false;
+        td = t;
+        ucur = cur;
+      } else {
+        const float2 l = cmul(cur, inv);
+        arow[t] = l;
+        if (t + 1 < w) cur = csub(nxt, cmul(l, csub(P[t + 1], cmul(lw, Fp[t + 1]))));
+        lprev = l;
+      }
+    }
+  }
+  if (td >= 0) {
+#pragma unroll
+    for (int c = 0; c < kPanelNB; ++c)
+      if (c > td && c < w) arow[c] = v[c];
+    arow[td] = ucur;
+  }
+  cluster.sync();
+  if (rank == 0 && wid == 0) {
+    replay_pivots(w, sh.perm, ipiv, ipiv_base, rowmap);
+    if (lane == 0 && sh.singular && info) atomicCAS(info, 0, ipiv_base + sh.singular);
+  }
+  if (tid == 0 && sh.timeout) {
+    if (status) atomicExch(status, BEM200_ERR_TIMEOUT);
+    else if (info) atomicExch(info, -BEM200_ERR_TIMEOUT);
+  }
+}
+
+// ----------------------------------------------------------------------------
 // Grid-wide panel for tall panels (more rows than a 16-CTA cluster holds):
 // one row per thread as in the push panel, CTAs spread over the whole GPU and
 // launched cooperatively (all resident), one grid barrier per column.  Each
@@ -1105,6 +1373,32 @@ static int panel_lu(const LaContext& ctx, int m, int w, C* A, long long ld, int 
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       BEM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, m, w, A, ld, col, rowmap, ipiv, ipiv_base, ctx.dinfo, R));
+      count_launch();
+      return BEM200_OK;
+    }
+  }
+  if constexpr (sizeof(C) == 8) {
+    if (m <= kAsyncMaxCluster * kAsyncThreads) {
+      // complex64: asynchronous push panel, 128 - 384 rows per CTA
+      const int cs = min(kAsyncMaxCluster, max(1, ceil_div(m, 128)));
+      const int R = ceil_div(m, cs);
+      const int threads = ceil_div(R, 32) * 32;
+      auto kern = panel_lu_async_kernel;
+      BEM_CUDA_CHECK(set_kernel_attrs_once(kern, 0, true));
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(cs, 1, 1);
+      cfg.blockDim = dim3(threads, 1, 1);
+      cfg.dynamicSmemBytes = 0;
+      cfg.stream = ctx.stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = cs;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      BEM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, m, w, reinterpret_cast<float2*>(A), ld, col, rowmap, ipiv,
+                                        ipiv_base, ctx.dinfo, ctx.dstatus, R));
       count_launch();
       return BEM200_OK;
     }

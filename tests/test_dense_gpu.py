@@ -220,13 +220,56 @@ def test_getrf_c64_tournament_pivoting(cuda, n):
     assert berr[0] < 1e-4 and berr[0] < 10 * berr[1] + 1e-7, berr
 
 
-def test_getrf_c64_tournament_zero_column(cuda):
-    """A zero column inside a tall complex64 tournament panel is reported as
-    a zero pivot."""
-    import torch
+@pytest.mark.parametrize("flags", [0, 2], ids=["async_panel", "tournament"])
+@pytest.mark.parametrize("zcol", [10, 700])
+def test_getrf_c64_zero_column(cuda, flags, zcol):
+    """A zero column inside a tall complex64 panel (the asynchronous push
+    panel, or a tournament panel) is reported as a zero pivot, also in a
+    later panel of the look-ahead schedule."""
     n = 1200
     A = (_rand(n, n, 41) + 3 * np.eye(n)).astype(np.complex64)
-    A[:, 10] = 0
+    A[:, zcol] = 0
     At = _t(A)
-    rowmap, ipiv, info = _getrf_ws(At, 1, flags=2)
-    assert int(info.item()) == 11
+    rowmap, ipiv, info = _getrf_ws(At, 1, flags=flags)
+    assert int(info.item()) == zcol + 1
+
+
+def test_getrf_c64_pivots_match_lapack(cuda):
+    """complex64 partial pivoting (asynchronous push panels, CUDA-core
+    updates) picks LAPACK cgetrf's pivots on a random 600 x 600 matrix, with
+    factors equal to cgetrf's to complex64 rounding.  (On larger random
+    matrices the two diverge at the first near-tie that rounding decides.)"""
+    n = 600
+    A = _rand(n, n, 500 + n).astype(np.complex64)
+    lu, piv = sla.lu_factor(A)
+    At = _t(A)
+    rowmap, ipiv, info = _getrf_ws(At, 0)
+    assert int(info.item()) == 0
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv)
+    got = At.cpu().numpy()[rowmap.cpu().numpy()]
+    assert np.max(np.abs(got - lu)) / np.max(np.abs(lu)) < 1e-4
+
+
+@pytest.mark.parametrize("engine", [0, 1])
+@pytest.mark.parametrize("n", [2000, 5768])
+def test_getrf_c64_partial_pivoting_factors(cuda, n, engine):
+    """complex64 look-ahead LU with asynchronous push panels: rowmap is a
+    permutation consistent with ipiv, every multiplier is bounded as partial
+    pivoting on |re| + |im| implies (|l| <= sqrt 2), and P A = L U holds to
+    complex64 rounding (CUDA-core and bf16x3 tensor-core updates)."""
+    A = _rand(n, n, 700 + n).astype(np.complex64)
+    At = _t(A)
+    rowmap, ipiv, info = _getrf_ws(At, engine)
+    assert int(info.item()) == 0
+    perm = rowmap.cpu().numpy()
+    assert sorted(perm.tolist()) == list(range(n))
+    order = np.arange(n)
+    for k, q in enumerate(ipiv.cpu().numpy()):       # LAPACK swaps replayed
+        order[[k, q]] = order[[q, k]]
+    np.testing.assert_array_equal(order, perm)
+    F = At.cpu().numpy()[perm].astype(np.complex128)
+    L = np.tril(F, -1) + np.eye(n)
+    U = np.triu(F)
+    assert np.max(np.abs(L)) <= np.sqrt(2) * (1 + 1e-5)
+    r = np.max(np.abs(A[perm].astype(np.complex128) - L @ U)) / np.max(np.abs(A))
+    assert r < (1e-3 if engine else 1e-4), r
