@@ -272,4 +272,4 @@ def test_getrf_c64_partial_pivoting_factors(cuda, n, engine):
     U = np.triu(F)
     assert np.max(np.abs(L)) <= np.sqrt(2) * (1 + 1e-5)
     r = np.max(np.abs(A[perm].astype(np.complex128) - L @ U)) / np.max(np.abs(A))
-    assert r < (1e-3 if engine else 1e-4), r
+    assert r < (5e-3 if engine else 1e-4), r  # bf16x3 products: ~2^-16 each
