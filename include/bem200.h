@@ -41,6 +41,7 @@ extern "C" {
 #define BEM200_ERR_UNSUPPORTED 4  /* configuration not implemented */
 #define BEM200_ERR_TIMEOUT 5      /* a bounded device-side wait gave up */
 #define BEM200_ERR_NOCONV 6       /* iterative refinement stopped above its tolerance */
+#define BEM200_ERR_PIVOTING 7     /* an LU without row exchanges met a column that needs one */
 
 #define BEM200_C128 0 /* complex double, 16 bytes per element */
 #define BEM200_C64 1  /* complex float, 8 bytes per element */
@@ -219,6 +220,14 @@ size_t bem200_gemm_workspace_size(int engine, int m, int n, int k);
  * width of the look-ahead schedule (multiple of 32 in [64, 1024]; 0 = 128). */
 #define BEM200_GETRF_PARTIAL_PIVOTING 1
 #define BEM200_GETRF_TOURNAMENT_PIVOTING 2
+/* BEM200_GETRF_DIAGONAL_PIVOTS: factor without the pivot search (blocked,
+ * no row exchanges) and check every column against partial pivoting's choice
+ * (|a_ij|_1 <= |a_jj|_1 for all i > j at step j).  A passing matrix gets
+ * LAPACK's partial-pivoting factors (ipiv[k] = k, rowmap = identity); a
+ * failing one sets *info = -BEM200_ERR_PIVOTING and leaves A unusable, so
+ * keep a copy and factor it again without the flag.  Needs ws of
+ * bem200_getrf_workspace_size bytes. */
+#define BEM200_GETRF_DIAGONAL_PIVOTS 4
 int bem200_getrf(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
                  int32_t* info, void* ws, size_t ws_bytes, void* stream);
 int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv,
@@ -278,7 +287,11 @@ int bem200_bem_init(int precision, int engine, int n, void* ws, int eps_per_face
                     int32_t* info_host, void* stream);
 /* bem200_bem_init with the LU tiling exposed (for the project's autotuner):
  * lu_flags as bem200_getrf_ex's (BEM200_GETRF_TOURNAMENT_PIVOTING: complex64
- * factors with tournament panels), lookahead_nb the block width of the
+ * factors with tournament panels; BEM200_GETRF_DIAGONAL_PIVOTS: the four
+ * LUs without the pivot search, checked -- the call then returns
+ * BEM200_ERR_PIVOTING when one of G1, G2, Delta, Sigma needs row exchanges,
+ * and the caller writes the slots again and repeats the call without the
+ * flag), lookahead_nb the block width of the
  * look-ahead LU schedule (a multiple of 32 in [64, 1024]; 0 = 128).
  * phase_ms (HOST, 4 floats, or NULL): stage timer (CUDA events on the
  * stream; the call then synchronises): LU(G1) || LU(G2) with Sigma1 || Sigma2,

@@ -18,6 +18,7 @@ C64 = 1
 ERR_SINGULAR = 3
 ERR_TIMEOUT = 5
 ERR_NOCONV = 6
+ERR_PIVOTING = 7
 
 _lib = None
 

@@ -75,6 +75,9 @@ def _excitation_rhs(p, exc, enei):
     return npol, phi, a, alpha, De
 
 
+_DIAGONAL_PIVOTS = 4  # BEM200_GETRF_DIAGONAL_PIVOTS
+
+
 class BEMRet:
     """Retarded BEM solver (reference class mnpbem/bem/bem_ret.py:138)."""
 
@@ -82,7 +85,7 @@ class BEMRet:
     needs = {"sim": "ret"}
 
     def __init__(self, p, enei=None, precision="fp64", engine="bf16x3", ir_tol=1e-12, ir_maxit=30, gmres_ir=True,
-                 gmres_maxit=200, lu_tiles=None, **options):
+                 gmres_maxit=200, lu_tiles=None, pivoting="auto", **options):
         torch = _torch()
         if p is None:
             raise ValueError("BEMRet: 'p' must be a ComParticle (or compatible particle object), got None.")
@@ -106,6 +109,13 @@ class BEMRet:
                                                            and 64 <= lu_tiles <= 1024)):
             raise ValueError("BEMRet: lu_tiles must be None, 'auto' or a look-ahead width (multiple of 32, 64-1024)")
         self.lu_tiles = lu_tiles
+        # "auto": LUs without the pivot search, checked against partial
+        # pivoting's choice, repeated with partial pivoting when a factor
+        # matrix needs row exchanges; "partial": always partial pivoting
+        if pivoting not in ("auto", "partial"):
+            raise ValueError("BEMRet: pivoting must be 'auto' or 'partial'")
+        self.pivoting = pivoting
+        self.last_pivoting = None
         # stage timer of init (profiling): set to (ctypes.c_float * 4)() to record the phases
         self._phase_buf = None
         self.last_init_phases_ms = None
@@ -173,16 +183,26 @@ class BEMRet:
         self.k = 2 * np.pi / enei
         self._eps(enei)
         s = nat.stream_ptr()
-        if self._prec == 0:
-            self._assemble_into_slots(enei, "c128")
-        else:
+        if self._prec == 1:
             self.g.bem_matrices(enei, dtype="c128", out=self._G128)
-            for src, dst in zip(self._G128, self._slots):
-                nat.call("bem200_convert_c128_c64", n * n, nat.ptr(src), ctypes.c_void_p(dst), s)
-        info = ctypes.c_int32(0)
-        nat.call("bem200_bem_init_ex", self._prec, _ENGINES[self.engine], n, nat.ptr(self._ws), self._eps_mode,
-                 self._e1p, self._e2p, nat.ptr(self._nvec), self.k, nat.ptr(self._gws), self._gws_bytes, 0,
-                 self._lookahead(), self._phase_buf, ctypes.byref(info), s)
+        modes = ["diagonal", "partial"] if self.pivoting == "auto" else ["partial"]
+        for mode in modes:
+            if self._prec == 0:
+                self._assemble_into_slots(enei, "c128")
+            else:
+                for src, dst in zip(self._G128, self._slots):
+                    nat.call("bem200_convert_c128_c64", n * n, nat.ptr(src), ctypes.c_void_p(dst), s)
+            info = ctypes.c_int32(0)
+            st = nat.lib().bem200_bem_init_ex(
+                self._prec, _ENGINES[self.engine], n, nat.ptr(self._ws), self._eps_mode, self._e1p, self._e2p,
+                nat.ptr(self._nvec), self.k, nat.ptr(self._gws), self._gws_bytes,
+                _DIAGONAL_PIVOTS if mode == "diagonal" else 0, self._lookahead(), self._phase_buf,
+                ctypes.byref(info), s)
+            if st == nat.ERR_PIVOTING and mode == "diagonal":
+                continue  # a factor matrix needs row exchanges: factor again with partial pivoting
+            nat.check(st, "bem200_bem_init_ex")
+            self.last_pivoting = mode
+            break
         if self._phase_buf is not None:
             self.last_init_phases_ms = list(self._phase_buf)
         self.enei = enei

@@ -818,14 +818,18 @@ int bem200_bem_init_ex(int precision, int engine, int n, void* ws, int eps_per_f
                        const double* eps2, const double* nvec, double k0, void* gemm_ws, size_t gemm_ws_bytes,
                        int lu_flags, int lookahead_nb, float* phase_ms, int32_t* info_host, void* stream) {
   BEM_REQUIRE(n > 0 && ws && eps1 && eps2 && nvec, BEM200_ERR_ARG, "bem_init: bad arguments");
-  BEM_REQUIRE((lu_flags & ~(BEM200_GETRF_PARTIAL_PIVOTING | BEM200_GETRF_TOURNAMENT_PIVOTING)) == 0, BEM200_ERR_ARG, "bem_init: unknown LU flags 0x%x",
-              lu_flags);
+  BEM_REQUIRE((lu_flags & ~(BEM200_GETRF_PARTIAL_PIVOTING | BEM200_GETRF_TOURNAMENT_PIVOTING |
+                             BEM200_GETRF_DIAGONAL_PIVOTS)) == 0,
+              BEM200_ERR_ARG, "bem_init: unknown LU flags 0x%x", lu_flags);
+  BEM_REQUIRE(!((lu_flags & BEM200_GETRF_DIAGONAL_PIVOTS) && (lu_flags & BEM200_GETRF_TOURNAMENT_PIVOTING)),
+              BEM200_ERR_ARG, "bem_init: diagonal and tournament pivoting exclude each other");
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
   ctx.engine = engine_from(engine);
   ctx.ws = gemm_ws;
   ctx.ws_bytes = gemm_ws_bytes;
   ctx.tournament = (lu_flags & BEM200_GETRF_TOURNAMENT_PIVOTING) && !(lu_flags & BEM200_GETRF_PARTIAL_PIVOTING);
+  ctx.diag_pivots = (lu_flags & BEM200_GETRF_DIAGONAL_PIVOTS) != 0;
   ctx.la_nb = lookahead_nb;
   EpsArg eps = make_eps(eps_per_face, eps1, eps2);
   StageTimer tm;
@@ -843,6 +847,9 @@ int bem200_bem_init_ex(int precision, int engine, int n, void* ws, int eps_per_f
     int* dinfo = precision == 0 ? state_view<double2>(n, ws).info : state_view<float2>(n, ws).info;
     BEM_CUDA_CHECK(cudaMemcpyAsync(info_host, dinfo, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
     BEM_CUDA_CHECK(cudaStreamSynchronize(ctx.stream));
+    BEM_REQUIRE(*info_host != -BEM200_ERR_PIVOTING, BEM200_ERR_PIVOTING,
+                "bem_init: a factor matrix needs row exchanges (factor it with partial pivoting)");
+    BEM_REQUIRE(*info_host != -BEM200_ERR_TIMEOUT, BEM200_ERR_TIMEOUT, "bem_init: a bounded device wait gave up");
     BEM_REQUIRE(*info_host == 0, BEM200_ERR_SINGULAR, "bem_init: exactly singular pivot at column %d", *info_host);
   }
   return BEM200_OK;

@@ -1350,9 +1350,112 @@ __global__ void __launch_bounds__(kCaluThreads, 1) panel_calu_kernel(int m, int 
   }
 }
 
+// ----------------------------------------------------------------------------
+// Panel without row exchanges, checked against partial pivoting (getrf with
+// ctx.diag_pivots).  Partial pivoting exchanges no rows when at every step j
+// the diagonal element is the first largest |re| + |im| of its column; the
+// factor matrices of the retarded BEM (G1, G2, Delta, mostly Sigma) have
+// that property, so their panels can skip the column-wide pivot search that
+// bounds the pivoted panels.  Every CTA factors the w x w diagonal block in
+// shared memory (warp 0, a lane per row), then each thread takes one row
+// below it through x U11 = a (forward substitution in registers, the
+// triangle fully unrolled).  Column j fails the check when some row has
+// |a_ij^(j)|_1 > tau |a_jj^(j)|_1; a failing panel raises ctx.vflag and the
+// caller factors the matrix again with partial pivoting.  With tau = 1 a
+// passing matrix gets LAPACK's partial-pivoting factors (no exchanges).
+constexpr int kNopivPanelThreads = 256;
+
+template <typename C>
+__global__ void __launch_bounds__(kNopivPanelThreads) panel_nopiv_kernel(int m, int w, C* __restrict__ A, long long ld,
+                                                                         int col, const int32_t* __restrict__ rowmap,
+                                                                         int32_t* __restrict__ ipiv, int ipiv_base,
+                                                                         int* __restrict__ info,
+                                                                         int* __restrict__ vflag, R_t<C> tau) {
+  __shared__ C D[kPanelNB][kPanelNB + 1];
+  __shared__ C rinv[kPanelNB];
+  __shared__ int zfirst, viol;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) {
+    zfirst = INT_MAX;
+    viol = 0;
+  }
+  for (int idx = tid; idx < w * w; idx += kNopivPanelThreads) {
+    const int i = idx / w, c = idx % w;
+    D[i][c] = A[(long long)rowmap[i] * ld + col + c];
+  }
+  __syncthreads();
+  if (wid == 0) {  // the diagonal block, lane i owning row i
+    bool bad = false;
+    for (int j = 0; j < w; ++j) {
+      const C piv = D[j][j];
+      const R_t<C> pm = pmag(piv);
+      const C inv = pm > 0 ? cdiv(cmake<C>(1.0, 0.0), piv) : czero<C>();
+      if (lane > j && lane < w) {
+        const C a = D[lane][j];
+        if (pmag(a) > tau * pm) bad = true;
+        const C l = cmul(a, inv);
+        D[lane][j] = l;
+        for (int c = j + 1; c < w; ++c) D[lane][c] = csub(D[lane][c], cmul(l, D[j][c]));
+      }
+      if (lane == 0 && !(pm > 0) && zfirst == INT_MAX) zfirst = j;
+      __syncwarp();
+    }
+    if (lane < w) {
+      const C d = D[lane][lane];
+      rinv[lane] = pmag(d) > 0 ? cdiv(cmake<C>(1.0, 0.0), d) : czero<C>();
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) viol = 1;
+  }
+  __syncthreads();
+  const int r = w + blockIdx.x * kNopivPanelThreads + tid;  // a logical row below the diagonal block
+  if (r < m) {
+    C* row = A + (long long)rowmap[r] * ld + col;
+    C x[kPanelNB];
+#pragma unroll
+    for (int c = 0; c < kPanelNB; ++c) x[c] = c < w ? row[c] : czero<C>();
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < kPanelNB; ++j) {
+      if (j < w) {
+        if (pmag(x[j]) > tau * pmag(D[j][j])) bad = true;  // x_j = a_rj^(j) here
+        const C l = cmul(x[j], rinv[j]);
+        x[j] = l;
+#pragma unroll
+        for (int c = j + 1; c < kPanelNB; ++c)
+          if (c < w) x[c] = csub(x[c], cmul(l, D[j][c]));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kPanelNB; ++c)
+      if (c < w) row[c] = x[c];
+    if (bad) viol = 1;
+  }
+  if (blockIdx.x == 0) {
+    for (int idx = tid; idx < w * w; idx += kNopivPanelThreads) {
+      const int i = idx / w, c = idx % w;
+      A[(long long)rowmap[i] * ld + col + c] = D[i][c];
+    }
+    if (tid < w) ipiv[tid] = ipiv_base + tid;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (viol && vflag) atomicExch(vflag, 1);
+    if (blockIdx.x == 0 && zfirst != INT_MAX && info) atomicCAS(info, 0, ipiv_base + zfirst + 1);
+  }
+}
+
 template <typename C>
 static int panel_lu(const LaContext& ctx, int m, int w, C* A, long long ld, int col, int32_t* rowmap, int32_t* ipiv,
                     int ipiv_base) {
+  if (ctx.diag_pivots) {
+    const int grid = max(1, ceil_div(m - w, kNopivPanelThreads));
+    panel_nopiv_kernel<C><<<grid, kNopivPanelThreads, 0, ctx.stream>>>(m, w, A, ld, col, rowmap, ipiv, ipiv_base,
+                                                                        ctx.dinfo, ctx.vflag,
+                                                                        (R_t<C>)ctx.pivot_tau);
+    BEM_LAUNCH_CHECK();
+    count_launch();
+    return BEM200_OK;
+  }
   if constexpr (sizeof(C) == 8) {
     if (ctx.tournament && m > kCaluMinRows && m <= kCaluMaxCluster * kCaluThreads) {
       // complex64: tournament pivoting, 128 - 512 rows per CTA
@@ -2138,9 +2241,36 @@ static int getrf_lookahead(const LaContext& ctx, int n, C* A, long long ld, int3
   return BEM200_OK;
 }
 
+__global__ void nopiv_finish_kernel(const int* __restrict__ vflag, int* __restrict__ info) {
+  if (*vflag) atomicExch(info, -BEM200_ERR_PIVOTING);
+}
+
+template <typename C>
+static int getrf_dispatch(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv,
+                          int32_t* scratch);
+
+// Checked diagonal pivots (ctx.diag_pivots): the same blocked look-ahead LU
+// with panel_nopiv panels; the panels' verdicts collect in a flag in the LU
+// scratch, turned into *info = -BEM200_ERR_PIVOTING at the end.
 template <typename C>
 int getrf(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv, int32_t* scratch) {
   BEM_REQUIRE(n > 0 && A && rowmap && ipiv && ld >= n, BEM200_ERR_ARG, "getrf: bad arguments");
+  if (!ctx.diag_pivots) return getrf_dispatch<C>(ctx, n, A, ld, rowmap, ipiv, scratch);
+  BEM_REQUIRE(scratch && ctx.dinfo, BEM200_ERR_ARG, "getrf: checked diagonal pivots need the LU workspace and info");
+  LaContext c = ctx;
+  c.vflag = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) +
+                                   (((size_t)2 * n * sizeof(int32_t) + 255) & ~size_t(255)));
+  BEM_CUDA_CHECK(cudaMemsetAsync(c.vflag, 0, sizeof(int), ctx.stream));
+  int st = getrf_dispatch<C>(c, n, A, ld, rowmap, ipiv, scratch);
+  if (st) return st;
+  nopiv_finish_kernel<<<1, 1, 0, ctx.stream>>>(c.vflag, ctx.dinfo);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+template <typename C>
+static int getrf_dispatch(const LaContext& ctx, int n, C* A, long long ld, int32_t* rowmap, int32_t* ipiv,
+                          int32_t* scratch) {
   // look-ahead needs the row-map snapshots (scratch) and, on the tensor-core
   // engines, room for two concurrent GEMMs in the operand workspace
   const bool ws_ok = ctx.engine == GemmEngine::kSimt ||
@@ -2467,7 +2597,11 @@ size_t bem200_getrf_workspace_size(int dtype, int engine, int n) {
 
 int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* rowmap, int32_t* ipiv, int32_t* info,
                     void* ws, size_t ws_bytes, int flags, int lookahead_nb, void* stream) {
-  BEM_REQUIRE((flags & ~(BEM200_GETRF_PARTIAL_PIVOTING | BEM200_GETRF_TOURNAMENT_PIVOTING)) == 0, BEM200_ERR_ARG, "getrf: unknown flags 0x%x", flags);
+  BEM_REQUIRE((flags & ~(BEM200_GETRF_PARTIAL_PIVOTING | BEM200_GETRF_TOURNAMENT_PIVOTING |
+                          BEM200_GETRF_DIAGONAL_PIVOTS)) == 0,
+              BEM200_ERR_ARG, "getrf: unknown flags 0x%x", flags);
+  BEM_REQUIRE(!((flags & BEM200_GETRF_DIAGONAL_PIVOTS) && (flags & BEM200_GETRF_TOURNAMENT_PIVOTING)),
+              BEM200_ERR_ARG, "getrf: diagonal and tournament pivoting exclude each other");
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
   ctx.engine = engine_of(engine);
@@ -2475,6 +2609,7 @@ int bem200_getrf_ex(int dtype, int engine, int n, void* A, int64_t ld, int32_t* 
   ctx.ws_bytes = ws_bytes;
   ctx.dinfo = info;
   ctx.tournament = (flags & BEM200_GETRF_TOURNAMENT_PIVOTING) && !(flags & BEM200_GETRF_PARTIAL_PIVOTING);
+  ctx.diag_pivots = (flags & BEM200_GETRF_DIAGONAL_PIVOTS) != 0;
   ctx.la_nb = lookahead_nb;
   int32_t* snap = nullptr;
   if (ws && n > 0 && ws_bytes >= bem200_getrf_workspace_size(dtype, engine, n)) {

@@ -61,9 +61,14 @@ struct LaContext {
   void* panel_ws = nullptr; // candidate slots of the grid-wide panel (panels of more rows than a cluster holds)
   bool tournament = false;  // complex64 panels: tournament pivoting (false: partial pivoting, LAPACK's pivots)
   int la_nb = 0;            // look-ahead block width of getrf (multiple of 32; 0 = 128)
+  bool diag_pivots = false; // getrf without the pivot search, checked against partial pivoting's choice
+  float pivot_tau = 1.0f;   // ... passing when |a_ij|_1 <= tau |a_jj|_1 (1: exactly LAPACK's pivots)
+  int* vflag = nullptr;     // device int raised by a panel that fails that check
 };
 
-// bytes of the grid-wide panel's candidate slots (2 x up to 160 CTAs x (32 + 1) complex128)
+// LU scratch beyond the row-map snapshots: the grid-wide panel's candidate
+// slots (2 x up to 160 CTAs x (32 + 1) complex128); with checked diagonal
+// pivots its first int is the panels' verdict flag
 constexpr size_t kPanelGridScratch = 176u * 1024u;
 
 // A non-blocking side stream forked from ctx.stream (fork()) and joined back

@@ -3,7 +3,7 @@
     python -m mnpbem_b200.microbench step  [--faces 1444] [--precision mixed|fp64] [--steps 1] [--warmup 1]
     python -m mnpbem_b200.microbench green [--faces 1444] [--dtype c128|c64] [--reps 3]
     python -m mnpbem_b200.microbench gemm  [--m 5768 --n 2884 --k 2884] [--engine 1] [--reps 3]
-    python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1] [--tournament]
+    python -m mnpbem_b200.microbench getrf [--n 5768] [--dtype c64] [--engine 1] [--reps 1] [--tournament | --diagonal]
     python -m mnpbem_b200.microbench hmat  [--faces 1444] [--cleaf 200] [--htol 1e-6] [--reps 3]
     python -m mnpbem_b200.microbench iter  [--faces 1444] [--hmatrix] [--noprecond] [--tol 1e-10]
     python -m mnpbem_b200.microbench large [--side 3 | --shape cube] [--hmatrix] [--tol 1e-8]
@@ -135,6 +135,8 @@ def case_getrf(a):
     code = nat.C128 if a.dtype == "c128" else nat.C64
     gen = torch.Generator(device="cuda").manual_seed(0)
     A0 = torch.randn(n, n, dtype=dt, device="cuda", generator=gen)
+    if a.diagonal:  # a column-dominant diagonal, as the BEM factor matrices have: no row exchanges
+        A0 += 100.0 * torch.eye(n, dtype=dt, device="cuda")
     A = torch.empty_like(A0)
     rowmap = torch.empty(n, dtype=torch.int32, device="cuda")
     ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -142,7 +144,7 @@ def case_getrf(a):
     wsb = int(nat.lib().bem200_getrf_workspace_size(code, a.engine, n))
     ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
 
-    flags = 2 if a.tournament else 0
+    flags = 2 if a.tournament else (4 if a.diagonal else 0)
 
     def go():
         A.copy_(A0)
@@ -169,7 +171,8 @@ def case_getrf(a):
     else:
         ms = _timed(go, a.reps)
     return {"case": "getrf", "n": n, "dtype": a.dtype, "engine": a.engine, "graph": bool(a.graph),
-            "pivoting": "tournament (complex64 panels > 512 rows)" if a.tournament else "partial", "ms": ms,
+            "pivoting": "tournament (complex64 panels > 512 rows)" if a.tournament else (
+                "diagonal (checked, no row exchanges)" if a.diagonal else "partial"), "ms": ms,
             "TFLOPs": 8.0 / 3.0 * n ** 3 / ms / 1e9, "info": int(info.item()), "backward_error": berr}
 
 
@@ -470,6 +473,8 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--graph", action="store_true", help="getrf: replay from a CUDA graph")
     ap.add_argument("--tournament", action="store_true", help="getrf: tournament pivoting of complex64 panels")
+    ap.add_argument("--diagonal", action="store_true",
+                    help="getrf: checked diagonal pivots (no pivot search) on a column-dominant matrix")
     ap.add_argument("--la-nb", dest="la_nb", type=int, default=0, help="getrf: look-ahead block width (0 = 128)")
     ap.add_argument("--cleaf", type=int, default=200)
     ap.add_argument("--htol", type=float, default=1e-6)

@@ -104,3 +104,31 @@ def test_operator_residual_of_fp64_solution(cuda):
     rn = float(torch.max(torch.abs(r)).item())
     bn = float(torch.max(torch.abs(b)).item())
     assert rn / bn < 1e-10
+
+
+def _cube_needing_exchanges():
+    """tricube(12, 60 nm): its Sigma at 600 nm needs one row exchange in a
+    partial-pivoting LU (G1, G2 and Delta need none)."""
+    from mnpbem_b200 import ComParticle, EpsConst, EpsDrude
+    from mnpbem_b200.geometry import tricube
+    return ComParticle([EpsConst(1.0), EpsDrude(9.84, 9.0, 0.067)], [tricube(12, 60.0, 0.25, interp="curv")],
+                       [[2, 1]], 1, interp="curv")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["dimer", "cube"])
+def test_checked_diagonal_pivots_equal_partial_pivoting(cuda, precision, case):
+    """pivoting='auto' factors G1, G2, Delta, Sigma without the pivot search
+    when partial pivoting would exchange no rows (the dimer at 520 nm) and
+    repeats the init with partial pivoting when one needs exchanges (the
+    cube's Sigma at 600 nm; the same dimer's Sigma at 620 nm needs one too);
+    either way the solution equals pivoting='partial''s."""
+    cp, enei = (dimer(), 520.0) if case == "dimer" else (_cube_needing_exchanges(), 600.0)
+    a_bem, a_sig, a_ext, a_sca = _run(cp, enei, precision=precision)
+    b_bem, b_sig, b_ext, b_sca = _run(cp, enei, precision=precision, pivoting="partial")
+    assert a_bem.last_pivoting == ("diagonal" if case == "dimer" else "partial")
+    assert b_bem.last_pivoting == "partial"
+    tol = 1e-12 if precision == "fp64" else 1e-10
+    assert abs(a_ext - b_ext) <= tol * abs(b_ext)
+    assert abs(a_sca - b_sca) <= tol * abs(b_sca)
+    assert rel(a_sig.sig2, b_sig.sig2) < 1e3 * tol

@@ -273,3 +273,75 @@ def test_getrf_c64_partial_pivoting_factors(cuda, n, engine):
     assert np.max(np.abs(L)) <= np.sqrt(2) * (1 + 1e-5)
     r = np.max(np.abs(A[perm].astype(np.complex128) - L @ U)) / np.max(np.abs(A))
     assert r < (5e-3 if engine else 1e-4), r  # bf16x3 products: ~2^-16 each
+
+
+def _dominant(n, seed, dt):
+    """A random matrix with a column-dominant diagonal: partial pivoting makes no row exchange."""
+    return (_rand(n, n, seed) + 4.0 * np.sqrt(n) * np.eye(n)).astype(dt)
+
+
+@pytest.mark.parametrize("n", [100, 1000, 2000])
+def test_getrf_diagonal_pivots_c128_equal_lapack(cuda, n):
+    """BEM200_GETRF_DIAGONAL_PIVOTS (no pivot search, blocked, checked): on a
+    matrix whose partial-pivoting LU exchanges no rows, LAPACK's pivots
+    (ipiv[k] = k) and its factors to FP64 rounding; block edges at n = 1000
+    (not a multiple of the 64-column blocks)."""
+    A = _dominant(n, 60 + n, np.complex128)
+    lu, piv = sla.lu_factor(A)
+    assert np.array_equal(piv, np.arange(n))
+    At = _t(A)
+    rowmap, ipiv, info = _getrf_ws(At, 0, flags=4)
+    assert int(info.item()) == 0
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv)
+    np.testing.assert_array_equal(rowmap.cpu().numpy(), np.arange(n))
+    assert np.max(np.abs(At.cpu().numpy() - lu)) / np.max(np.abs(lu)) < 1e-12
+
+
+@pytest.mark.parametrize("engine", [0, 1])
+@pytest.mark.parametrize("n", [300, 1000, 5768])
+def test_getrf_diagonal_pivots_c64_equal_partial(cuda, n, engine):
+    """complex64 checked diagonal pivots (128-column blocks, tensor-core or
+    CUDA-core trailing updates) against the partial-pivoting LU of the same
+    matrix (which exchanges no rows): same pivots, factors equal to complex64
+    rounding, and a solve as accurate."""
+    A = _dominant(n, 80 + n, np.complex64)
+    ref = _t(A)
+    rmap, rpiv, rinfo = _getrf_ws(ref, engine)
+    assert int(rinfo.item()) == 0 and np.array_equal(rpiv.cpu().numpy(), np.arange(n))
+    At = _t(A)
+    rowmap, ipiv, info = _getrf_ws(At, engine, flags=4)
+    assert int(info.item()) == 0
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), np.arange(n))
+    F, R = At.cpu().numpy(), ref.cpu().numpy()[rmap.cpu().numpy()]
+    assert np.max(np.abs(F - R)) / np.max(np.abs(R)) < (2e-4 if engine else 2e-5)
+    B = _rand(n, 2, 81 + n).astype(np.complex64)
+    Bt = _t(B)
+    getrs(At, rowmap, Bt)
+    X = np.linalg.solve(A.astype(np.complex128), B)
+    assert np.max(np.abs(Bt.cpu().numpy() - X)) / np.max(np.abs(X)) < 1e-4
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64])
+@pytest.mark.parametrize("where,off", [(3, 40), (3, 150), (700, 150)])
+def test_getrf_diagonal_pivots_report_needed_exchange(cuda, dt, where, off):
+    """A column whose partial-pivoting step would exchange rows -- with a row
+    of the same diagonal block, or with a row below it, in the first block or
+    a later one -- makes the checked LU report -BEM200_ERR_PIVOTING."""
+    n = 1000
+    A = _dominant(n, 90, dt)
+    A[[where, where + off]] = A[[where + off, where]]   # the diagonal of row `where` moves below it
+    At = _t(A)
+    _, _, info = _getrf_ws(At, 1 if dt == np.complex64 else 0, flags=4)
+    assert int(info.item()) == -nat.ERR_PIVOTING
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64])
+def test_getrf_diagonal_pivots_zero_column(cuda, dt):
+    """An all-zero column needs no exchange under partial pivoting either:
+    the checked LU reports the zero pivot (info = column + 1), as LAPACK."""
+    n = 500
+    A = _dominant(n, 91, dt)
+    A[:, 200] = 0
+    At = _t(A)
+    _, _, info = _getrf_ws(At, 0, flags=4)
+    assert int(info.item()) == 201
