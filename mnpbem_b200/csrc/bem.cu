@@ -113,6 +113,16 @@ __global__ void sigma_kernel(int n, const C* __restrict__ S1, const C* __restric
   S[idx] = to_c<C>(v);
 }
 
+// *info = -BEM200_ERR_PIVOTING if a check of a factorisation without row
+// exchanges raised *vflag
+__global__ void flag_to_info_kernel(const int* __restrict__ vflag, int* __restrict__ info) {
+  if (*vflag) atomicExch(info, -BEM200_ERR_PIVOTING);
+}
+
+// probe tolerance of the complex64 Delta^-1 (relative to max|v|): the
+// factors only precondition the FP64 refinement
+constexpr double kDeltaProbeTol = 1e-2;
+
 // The factor chains of G1 and G2 are independent: LU(G2) and Sigma2 run on a
 // second (non-blocking) stream forked from the caller's stream with events, so
 // the latency-bound panel factorisations of the two chains overlap.  Each
@@ -190,12 +200,32 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
     c.ws_bytes = ctx.ws_bytes;
   }
   if ((st = mark(1))) return st;
-  // Delta = Sigma1 - Sigma2, LU(Delta), Delta^-1
-  delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[4]);
-  BEM_LAUNCH_CHECK();
-  if ((st = getrf<C>(c, n, s.M[4], n, s.map[2], s.ipiv[2], s.snap[0]))) return st;
-  if ((st = mark(2))) return st;
-  if ((st = inverse<C>(c, n, s.M[4], n, s.map[2], s.M[5], n))) return st;
+  // Delta = Sigma1 - Sigma2, Delta^-1
+  bool inverted = false;
+  if constexpr (sizeof(C) == 8) {
+    if (ctx.diag_pivots && inverse_nopiv_scratch_elems<C>(n) <= (size_t)n * n) {
+      // complex64 with checked diagonal pivots: Delta^-1 by the block Schur
+      // complement (GEMMs) instead of LU(Delta) + two n-column triangular
+      // solves; a failed probe raises the pivoting flag (-> partial pivoting)
+      int* vflag = reinterpret_cast<int*>(reinterpret_cast<char*>(s.snap[0]) +
+                                          align256(sizeof(int32_t) * 2 * (size_t)n));
+      BEM_CUDA_CHECK(cudaMemsetAsync(vflag, 0, sizeof(int), ctx.stream));
+      delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[5]);
+      BEM_LAUNCH_CHECK();
+      if ((st = mark(2))) return st;
+      if ((st = inverse_nopiv<C>(c, n, s.M[5], n, s.M[4], vflag, kDeltaProbeTol))) return st;
+      flag_to_info_kernel<<<1, 1, 0, ctx.stream>>>(vflag, s.info);
+      BEM_LAUNCH_CHECK();
+      inverted = true;
+    }
+  }
+  if (!inverted) {
+    delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[4]);
+    BEM_LAUNCH_CHECK();
+    if ((st = getrf<C>(c, n, s.M[4], n, s.map[2], s.ipiv[2], s.snap[0]))) return st;
+    if ((st = mark(2))) return st;
+    if ((st = inverse<C>(c, n, s.M[4], n, s.map[2], s.M[5], n))) return st;
+  }
   if ((st = mark(3))) return st;
   // Sigma, LU(Sigma)
   sigma_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(n, s.M[2], s.M[3], s.M[5], nvec, eps, k0 * k0, s.M[6]);

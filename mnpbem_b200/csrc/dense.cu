@@ -1357,13 +1357,26 @@ __global__ void __launch_bounds__(kCaluThreads, 1) panel_calu_kernel(int m, int 
 // factor matrices of the retarded BEM (G1, G2, Delta, mostly Sigma) have
 // that property, so their panels can skip the column-wide pivot search that
 // bounds the pivoted panels.  Every CTA factors the w x w diagonal block in
-// shared memory (warp 0, a lane per row), then each thread takes one row
+// registers (warp 0, a lane per row), then each thread takes one row
 // below it through x U11 = a (forward substitution in registers, the
 // triangle fully unrolled).  Column j fails the check when some row has
 // |a_ij^(j)|_1 > tau |a_jj^(j)|_1; a failing panel raises ctx.vflag and the
 // caller factors the matrix again with partial pivoting.  With tau = 1 a
 // passing matrix gets LAPACK's partial-pivoting factors (no exchanges).
-constexpr int kNopivPanelThreads = 256;
+constexpr int kNopivPanelThreads = 64;
+
+// 1 / p for p != 0 (0 for p = 0), scaled by max(|re|, |im|) so that |p|^2
+// neither overflows nor underflows: two real divisions, no branches
+template <typename C>
+__device__ __forceinline__ C crecip_scaled(C p) {
+  using R = R_t<C>;
+  const R sc = fmax(fabs(p.x), fabs(p.y));
+  if (!(sc > R(0))) return czero<C>();
+  const R rs = R(1) / sc;
+  const R px = p.x * rs, py = p.y * rs;
+  const R f = rs / (px * px + py * py);
+  return cmake<C>(px * f, -py * f);
+}
 
 template <typename C>
 __global__ void __launch_bounds__(kNopivPanelThreads) panel_nopiv_kernel(int m, int w, C* __restrict__ A, long long ld,
@@ -1371,8 +1384,9 @@ __global__ void __launch_bounds__(kNopivPanelThreads) panel_nopiv_kernel(int m, 
                                                                          int32_t* __restrict__ ipiv, int ipiv_base,
                                                                          int* __restrict__ info,
                                                                          int* __restrict__ vflag, R_t<C> tau) {
-  __shared__ C D[kPanelNB][kPanelNB + 1];
-  __shared__ C rinv[kPanelNB];
+  // D is one row taller than the block: the rotated reads D[j][j + c] stay inside
+  __shared__ C D[kPanelNB + 1][kPanelNB + 1];
+  __shared__ C rinv[kPanelNB], prow[kPanelNB];
   __shared__ int zfirst, viol;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   if (tid == 0) {
@@ -1383,47 +1397,78 @@ __global__ void __launch_bounds__(kNopivPanelThreads) panel_nopiv_kernel(int m, 
     const int i = idx / w, c = idx % w;
     D[i][c] = A[(long long)rowmap[i] * ld + col + c];
   }
+  // this thread's row below the diagonal block (complex64: loaded while warp
+  // 0 factors the block; complex128 registers hold one row at a time)
+  const int r = w + blockIdx.x * kNopivPanelThreads + tid;
+  C* row = r < m ? A + (long long)rowmap[r] * ld + col : nullptr;
+  C x[kPanelNB];
+  if constexpr (sizeof(C) == 8) {
+#pragma unroll
+    for (int c = 0; c < kPanelNB; ++c) x[c] = (row && c < w) ? row[c] : czero<C>();
+  }
   __syncthreads();
-  if (wid == 0) {  // the diagonal block, lane i owning row i
+  // Both parts keep the current column in register 0: every step shifts the
+  // row left by one (updating the columns still open) and appends the new
+  // multiplier, so register indices stay static in a rolled loop; after the
+  // 32 steps of a full cycle the row is back in column order.
+  if (wid == 0) {  // the diagonal block, lane i owning row i (padded with the identity)
+    C v[kPanelNB];
+#pragma unroll
+    for (int c = 0; c < kPanelNB; ++c)
+      v[c] = (lane < w && c < w) ? D[lane][c] : (lane == c ? cmake<C>(1.0, 0.0) : czero<C>());
     bool bad = false;
-    for (int j = 0; j < w; ++j) {
-      const C piv = D[j][j];
-      const R_t<C> pm = pmag(piv);
-      const C inv = pm > 0 ? cdiv(cmake<C>(1.0, 0.0), piv) : czero<C>();
-      if (lane > j && lane < w) {
-        const C a = D[lane][j];
-        if (pmag(a) > tau * pm) bad = true;
-        const C l = cmul(a, inv);
-        D[lane][j] = l;
-        for (int c = j + 1; c < w; ++c) D[lane][c] = csub(D[lane][c], cmul(l, D[j][c]));
+#pragma unroll 1
+    for (int j = 0; j < kPanelNB; ++j) {
+      if (lane == j) {
+#pragma unroll
+        for (int c = 0; c < kPanelNB; ++c) prow[c] = v[c];
       }
-      if (lane == 0 && !(pm > 0) && zfirst == INT_MAX) zfirst = j;
+      __syncwarp();
+      const C piv = prow[0];
+      const R_t<C> pm = pmag(piv);
+      const C inv = crecip_scaled(piv);
+      const bool act = lane > j;
+      if (act && pmag(v[0]) > tau * pm) bad = true;
+      const C l = cmul(v[0], inv);
+      const C first = v[0];
+      const int lim = kPanelNB - 1 - j;
+#pragma unroll
+      for (int c = 1; c < kPanelNB; ++c) {
+        const C u = csub(v[c], cmul(l, prow[c]));
+        v[c - 1] = (act && c <= lim) ? u : v[c];
+      }
+      v[kPanelNB - 1] = act ? l : first;
+      if (lane == 0 && j < w && !(pm > 0) && zfirst == INT_MAX) zfirst = j;
       __syncwarp();
     }
-    if (lane < w) {
-      const C d = D[lane][lane];
-      rinv[lane] = pmag(d) > 0 ? cdiv(cmake<C>(1.0, 0.0), d) : czero<C>();
-    }
+#pragma unroll
+    for (int c = 0; c < kPanelNB; ++c) D[lane][c] = v[c];
+    C d = v[0];
+#pragma unroll
+    for (int c = 1; c < kPanelNB; ++c)
+      if (c == lane) d = v[c];
+    rinv[lane] = crecip_scaled(d);
     if (__any_sync(0xffffffffu, bad) && lane == 0) viol = 1;
   }
   __syncthreads();
-  const int r = w + blockIdx.x * kNopivPanelThreads + tid;  // a logical row below the diagonal block
-  if (r < m) {
-    C* row = A + (long long)rowmap[r] * ld + col;
-    C x[kPanelNB];
+  if constexpr (sizeof(C) == 16) {
 #pragma unroll
-    for (int c = 0; c < kPanelNB; ++c) x[c] = c < w ? row[c] : czero<C>();
+    for (int c = 0; c < kPanelNB; ++c) x[c] = (row && c < w) ? row[c] : czero<C>();
+  }
+  if (row) {  // x U11 = a; padded steps j >= w see an identity pivot and leave x alone
     bool bad = false;
-#pragma unroll
+#pragma unroll 1
     for (int j = 0; j < kPanelNB; ++j) {
-      if (j < w) {
-        if (pmag(x[j]) > tau * pmag(D[j][j])) bad = true;  // x_j = a_rj^(j) here
-        const C l = cmul(x[j], rinv[j]);
-        x[j] = l;
+      const C* Dj = &D[j][j];
+      if (pmag(x[0]) > tau * pmag(Dj[0])) bad = true;  // x[0] = a_rj^(j) here
+      const C l = cmul(x[0], rinv[j]);
+      const int lim = kPanelNB - 1 - j;
 #pragma unroll
-        for (int c = j + 1; c < kPanelNB; ++c)
-          if (c < w) x[c] = csub(x[c], cmul(l, D[j][c]));
+      for (int c = 1; c < kPanelNB; ++c) {
+        const C u = csub(x[c], cmul(l, Dj[c]));
+        x[c - 1] = c <= lim ? u : x[c];
       }
+      x[kPanelNB - 1] = l;
     }
 #pragma unroll
     for (int c = 0; c < kPanelNB; ++c)
@@ -2532,6 +2577,194 @@ int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_
   return BEM200_OK;
 }
 
+// ===================================================================== inverse without pivoting
+// M <- M^-1 in place by the block Schur complement, for matrices whose
+// partial-pivoting LU exchanges no rows (the retarded BEM's Delta):
+//   A^-1 (recursive), T1 = A^-1 B, T2 = C A^-1, S = D - C T1, S^-1 (recursive),
+//   B <- -T1 S^-1, C <- -S^-1 T2, A <- A^-1 - B T2.
+// Nearly all of the 8 n^3 flops land in the large GEMMs of the top levels
+// (tensor cores for complex64); the leaves (<= 64 x 64) are inverted by
+// Gauss-Jordan elimination in registers.  No row exchanges means no check
+// of the leaves' pivots can cover the rows outside them, so the caller
+// verifies the result with inverse_probe (M^-1 (M v) = v for a fixed
+// pseudo-random v) and falls back to the pivoted LU when it fails.
+constexpr int kInvLeaf = 64;
+constexpr int kInvLeafThreads = 256;
+
+// Gauss-Jordan inversion of the nb x nb (nb <= 64) block at M, in place.
+// Thread (ty, tx) of the 8 x 32 grid owns rows ty + 8 p, columns tx + 32 q
+// of a 64 x 64 tile padded with the identity; each step publishes the pivot
+// row and column through shared memory (double buffered: one barrier per
+// step).  A pivot that is not the first largest |re| + |im| among the rows
+// still to be eliminated, or is zero, raises *vflag.
+template <typename C>
+__global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __restrict__ M, long long ld,
+                                                                   R_t<C> tau, int* __restrict__ vflag) {
+  constexpr int PR = kInvLeaf / 8, QC = kInvLeaf / 32;
+  __shared__ C colb[2][kInvLeaf], rowb[2][kInvLeaf];
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  C a[PR][QC];
+#pragma unroll
+  for (int p = 0; p < PR; ++p)
+#pragma unroll
+    for (int q = 0; q < QC; ++q) {
+      const int i = ty + 8 * p, c = tx + 32 * q;
+      a[p][q] = (i < nb && c < nb) ? M[(long long)i * ld + c] : (i == c ? cmake<C>(1.0, 0.0) : czero<C>());
+    }
+  bool bad = false;
+#pragma unroll
+  for (int kp = 0; kp < PR; ++kp) {
+    const int qk = kp / 4;
+#pragma unroll 1
+    for (int kr = 0; kr < 8; ++kr) {
+      const int k = 8 * kp + kr, b = k & 1;
+      if (tx == (k & 31)) {
+#pragma unroll
+        for (int p = 0; p < PR; ++p) colb[b][ty + 8 * p] = a[p][qk];
+      }
+      if (ty == kr) {
+#pragma unroll
+        for (int q = 0; q < QC; ++q) rowb[b][tx + 32 * q] = a[kp][q];
+      }
+      __syncthreads();
+      const C piv = rowb[b][k];
+      const R_t<C> pm = pmag(piv);
+      const C pinv = crecip_scaled(piv);
+      if (k < nb && !(pm > 0)) bad = true;
+#pragma unroll
+      for (int p = 0; p < PR; ++p) {
+        const int i = ty + 8 * p;
+        const C aik = colb[b][i];
+        if (i > k && pmag(aik) > tau * pm) bad = true;
+        const C f = cmul(aik, pinv);
+        if (p == kp && ty == kr) {  // the pivot row
+#pragma unroll
+          for (int q = 0; q < QC; ++q) a[p][q] = (tx + 32 * q == k) ? pinv : cmul(a[p][q], pinv);
+        } else {
+#pragma unroll
+          for (int q = 0; q < QC; ++q)
+            a[p][q] = (tx + 32 * q == k) ? csub(czero<C>(), f) : csub(a[p][q], cmul(f, rowb[b][tx + 32 * q]));
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < PR; ++p)
+#pragma unroll
+    for (int q = 0; q < QC; ++q) {
+      const int i = ty + 8 * p, c = tx + 32 * q;
+      if (i < nb && c < nb) M[(long long)i * ld + c] = a[p][q];
+    }
+  if (__any_sync(0xffffffffu, bad) && tx == 0 && vflag) atomicExch(vflag, 1);
+}
+
+// scratch elements inverse_nopiv needs for an n x n matrix
+static size_t inverse_nopiv_scratch(int n) {
+  size_t total = 0;
+  while (n > kInvLeaf) {
+    const int n1 = min(n - 1, ceil_div(n / 2, kInvLeaf) * kInvLeaf), n2 = n - n1;
+    total += 2 * (size_t)n1 * n2;
+    n = n2;
+  }
+  return total;
+}
+
+template <typename C>
+static int inverse_nopiv_rec(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag) {
+  if (n <= kInvLeaf) {
+    inv_leaf_kernel<C><<<1, kInvLeafThreads, 0, ctx.stream>>>(n, M, ld, (R_t<C>)ctx.pivot_tau, vflag);
+    BEM_LAUNCH_CHECK();
+    count_launch();
+    return BEM200_OK;
+  }
+  const int n1 = min(n - 1, ceil_div(n / 2, kInvLeaf) * kInvLeaf), n2 = n - n1;
+  C* A = M;
+  C* B = M + n1;
+  C* Cm = M + (long long)n1 * ld;
+  C* D = Cm + n1;
+  int st;
+  if ((st = inverse_nopiv_rec<C>(ctx, n1, A, ld, ws, vflag))) return st;
+  C* T1 = ws;                            // n1 x n2
+  C* T2 = ws + (size_t)n1 * n2;          // n2 x n1
+  C* rest = T2 + (size_t)n2 * n1;
+  const C one = cmake<C>(1.0, 0.0), mone = cmake<C>(-1.0, 0.0), zero = czero<C>();
+  if ((st = gemm<C>(ctx, n1, n2, n1, one, A, ld, B, ld, zero, T1, n2))) return st;
+  if ((st = gemm<C>(ctx, n2, n1, n1, one, Cm, ld, A, ld, zero, T2, n1))) return st;
+  if ((st = gemm<C>(ctx, n2, n2, n1, mone, Cm, ld, T1, n2, one, D, ld))) return st;
+  if ((st = inverse_nopiv_rec<C>(ctx, n2, D, ld, rest, vflag))) return st;
+  if ((st = gemm<C>(ctx, n1, n2, n2, mone, T1, n2, D, ld, zero, B, ld))) return st;
+  if ((st = gemm<C>(ctx, n2, n1, n2, mone, D, ld, T2, n1, zero, Cm, ld))) return st;
+  return gemm<C>(ctx, n1, n1, n2, mone, B, ld, T2, n1, one, A, ld);
+}
+
+// v: n fixed pseudo-random complex values in [-1, 1) (a hash of the index)
+template <typename C>
+__global__ void probe_fill_kernel(int n, C* __restrict__ v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t h = (uint32_t)i * 2654435761u + 0x9e3779b9u;
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  const uint32_t g = h * 0xc2b2ae35u;
+  v[i] = cmake<C>((double)(h & 0xffffu) / 32768.0 - 1.0, (double)(g >> 16) / 32768.0 - 1.0);
+}
+
+// *vflag = 1 unless max|z - v| <= tol max|v|
+template <typename C>
+__global__ void __launch_bounds__(1024) probe_check_kernel(int n, const C* __restrict__ v, const C* __restrict__ z,
+                                                           double tol, int* __restrict__ vflag) {
+  __shared__ double se[32], sv[32];
+  double e = 0, m = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const C d = csub(z[i], v[i]);
+    const double de = fabs((double)d.x) + fabs((double)d.y);
+    e = fmax(e, de == de ? de : INFINITY);
+    m = fmax(m, fabs((double)v[i].x) + fabs((double)v[i].y));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    se[threadIdx.x >> 5] = e;
+    sv[threadIdx.x >> 5] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    e = threadIdx.x < (blockDim.x >> 5) ? se[threadIdx.x] : 0.0;
+    m = threadIdx.x < (blockDim.x >> 5) ? sv[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    if (threadIdx.x == 0 && !(e <= tol * m)) atomicExch(vflag, 1);
+  }
+}
+
+template <typename C>
+size_t inverse_nopiv_scratch_elems(int n) {
+  return inverse_nopiv_scratch(n) + 3 * (size_t)n + 64;
+}
+
+template <typename C>
+int inverse_nopiv(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag, double tol) {
+  BEM_REQUIRE(n > 0 && M && ws && vflag, BEM200_ERR_ARG, "inverse_nopiv: bad arguments");
+  C* v = ws + inverse_nopiv_scratch(n) + 32;
+  C* y = v + n;
+  C* z = y + n;
+  const C one = cmake<C>(1.0, 0.0), zero = czero<C>();
+  probe_fill_kernel<C><<<ceil_div(n, 256), 256, 0, ctx.stream>>>(n, v);
+  BEM_LAUNCH_CHECK();
+  int st;
+  if ((st = gemm<C>(ctx, n, 1, n, one, M, ld, v, 1, zero, y, 1))) return st;  // y = M v
+  if ((st = inverse_nopiv_rec<C>(ctx, n, M, ld, ws, vflag))) return st;
+  if ((st = gemm<C>(ctx, n, 1, n, one, M, ld, y, 1, zero, z, 1))) return st;  // z = M^-1 y
+  probe_check_kernel<C><<<1, 1024, 0, ctx.stream>>>(n, v, z, tol, vflag);
+  BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
 // explicit instantiations
 #define BEM_INST(C)                                                                                              \
   template int gemm_v<C>(const LaContext&, int, int, int, C, RowView<C>, RowView<C>, C, RowView<C>);             \
@@ -2543,6 +2776,8 @@ int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_
   template int trsv_diag_inverse<C>(const LaContext&, int, const C*, long long, const int32_t*, C*, C*);         \
   template int solve_right<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long, C*); \
   template int inverse<C>(const LaContext&, int, const C*, long long, const int32_t*, C*, long long);         \
+  template size_t inverse_nopiv_scratch_elems<C>(int);                                                          \
+  template int inverse_nopiv<C>(const LaContext&, int, C*, long long, C*, int*, double);                       \
   template int solve_left_T<C>(const LaContext&, int, int, const C*, long long, const int32_t*, C*, long long,   \
                                void*);                                                                           \
   template size_t gemm_t_scratch_bytes<C>(int, int);                                                             \

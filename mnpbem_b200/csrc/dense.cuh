@@ -166,6 +166,16 @@ int solve_right(const LaContext& ctx, int n, int m, const C* LU, long long ld, c
 template <typename C>
 int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_t* rowmap, C* Inv, long long ldi);
 
+// M <- M^-1 in place without pivoting (block Schur complement, Gauss-Jordan
+// leaves), verified by a probe: *vflag (device int) is raised when
+// M^-1 (M v) differs from v by more than tol max|v| for a fixed pseudo-random
+// v, or a leaf pivot is zero or not partial pivoting's choice; M is then
+// unusable.  ws: inverse_nopiv_scratch_elems(n) elements.
+template <typename C>
+size_t inverse_nopiv_scratch_elems(int n);
+template <typename C>
+int inverse_nopiv(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag, double tol);
+
 // bytes of scratch the tensor-core GEMM needs for an m x n x k product
 size_t gemm_tc_workspace(int m, int n, int k, GemmEngine e);
 int gemm_tc_c64(const LaContext& ctx, int m, int n, int k, float2 alpha, RowView<float2> A, RowView<float2> B,
