@@ -35,12 +35,13 @@ __device__ __forceinline__ C shfl_c(C v, int src) {
 }
 
 // ===================================================================== GEMM
-// C = alpha A B + beta C on row views; block tile 64 x 64, each thread a 4 x 4
-// register tile (rows ty + 16 i, cols tx + 16 j).
-template <typename C, int BK>
+// C = alpha A B + beta C on row views; block tile (16 TM) x (16 TM), each
+// thread a TM x TM register tile (rows ty + 16 i, cols tx + 16 j).  TM = 4
+// for most shapes, TM = 2 when 64 x 64 tiles would leave most SMs idle.
+template <typename C, int BK, int TM = 4>
 __global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C alpha, RowView<C> A, RowView<C> B,
                                                         C beta, RowView<C> Cv) {
-  constexpr int BM = 64, BN = 64;
+  constexpr int BM = 16 * TM, BN = 16 * TM;
   constexpr int A_LOADS = BM * BK / 256;  // rows of A loaded per thread (fixed over k)
   constexpr int B_LOADS = BK * BN / 256;
   __shared__ C As[BK][BM + 1];
@@ -58,11 +59,11 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C a
   }
   const int bc = tid % BN, br0 = tid / BN;
   const bool bcol_ok = (n0 + bc) < n;
-  C acc[4][4];
+  C acc[TM][TM];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < TM; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = czero<C>();
+    for (int j = 0; j < TM; ++j) acc[i][j] = czero<C>();
   for (int k0 = 0; k0 < k; k0 += BK) {
     const bool kfull = (k0 + BK) <= k;
     const int gc = k0 + ac;
@@ -77,15 +78,15 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C a
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      C a[4], b[4];
+      C a[TM], b[TM];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+      for (int i = 0; i < TM; ++i) a[i] = As[kk][ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+      for (int j = 0; j < TM; ++j) b[j] = Bs[kk][tx + 16 * j];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < TM; ++j) {
           acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
           acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
           acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
@@ -96,12 +97,12 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C a
   }
   const bool use_beta = (beta.x != 0 || beta.y != 0);
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < TM; ++i) {
     int gr = m0 + ty + 16 * i;
     if (gr >= m) continue;
     const long long roff = Cv.off(gr, 0);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < TM; ++j) {
       int gc = n0 + tx + 16 * j;
       if (gc >= n) continue;
       C v = cmul(alpha, acc[i][j]);
@@ -192,6 +193,8 @@ static int gemm_skinny(const LaContext& ctx, int m, int n, int k, C alpha, RowVi
   return BEM200_OK;
 }
 
+constexpr double kTcMinMacs = 268435456.0;  // 2^28
+
 template <typename C>
 int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv) {
   if (m <= 0 || n <= 0) return BEM200_OK;
@@ -202,12 +205,22 @@ int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, Row
     return gemm_skinny<C, 16, kRw16>(ctx, m, n, k, alpha, A, B, beta, Cv);
   }
   if constexpr (sizeof(C) == 8) {
-    if (ctx.engine != GemmEngine::kSimt && k >= 64 && m >= 128 && n >= 64)
+    // the tensor-core path pays ~15 us of operand preparation and pipeline
+    // fill per call: below ~2^28 multiply-adds the CUDA-core tiles finish first
+    if (ctx.engine != GemmEngine::kSimt && k >= 64 && m >= 128 && n >= 64 &&
+        (double)m * n * k >= kTcMinMacs)
       return gemm_tc_c64(ctx, m, n, k, alpha, A, B, beta, Cv);
+  }
+  constexpr int BK = sizeof(C) == 16 ? 8 : 16;
+  if ((long long)ceil_div(n, 64) * ceil_div(m, 64) < 296) {  // fewer than two 64 x 64 tiles per SM
+    dim3 grid(ceil_div(n, 32), ceil_div(m, 32));
+    BEM_REQUIRE(grid.y <= 65535, BEM200_ERR_ARG, "gemm: m too large");
+    gemm_simt_kernel<C, BK, 2><<<grid, 256, 0, ctx.stream>>>(m, n, k, alpha, A, B, beta, Cv);
+    BEM_LAUNCH_CHECK();
+    return BEM200_OK;
   }
   dim3 grid(ceil_div(n, 64), ceil_div(m, 64));
   BEM_REQUIRE(grid.y <= 65535, BEM200_ERR_ARG, "gemm: m too large");
-  constexpr int BK = sizeof(C) == 16 ? 8 : 16;
   gemm_simt_kernel<C, BK><<<grid, 256, 0, ctx.stream>>>(m, n, k, alpha, A, B, beta, Cv);
   BEM_LAUNCH_CHECK();
   return BEM200_OK;
@@ -2583,25 +2596,35 @@ int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_
 //   A^-1 (recursive), T1 = A^-1 B, T2 = C A^-1, S = D - C T1, S^-1 (recursive),
 //   B <- -T1 S^-1, C <- -S^-1 T2, A <- A^-1 - B T2.
 // Nearly all of the 8 n^3 flops land in the large GEMMs of the top levels
-// (tensor cores for complex64); the leaves (<= 64 x 64) are inverted by
+// (tensor cores for complex64); the leaves (<= 128 x 128 complex64, 64 x 64
+// complex128) are inverted by
 // Gauss-Jordan elimination in registers.  No row exchanges means no check
 // of the leaves' pivots can cover the rows outside them, so the caller
 // verifies the result with inverse_probe (M^-1 (M v) = v for a fixed
 // pseudo-random v) and falls back to the pivoted LU when it fails.
-constexpr int kInvLeaf = 64;
+template <typename C> struct InvLeaf { static constexpr int value = 128; };
+template <> struct InvLeaf<double2> { static constexpr int value = 64; };
 constexpr int kInvLeafThreads = 256;
 
-// Gauss-Jordan inversion of the nb x nb (nb <= 64) block at M, in place.
-// Thread (ty, tx) of the 8 x 32 grid owns rows ty + 8 p, columns tx + 32 q
-// of a 64 x 64 tile padded with the identity; each step publishes the pivot
-// row and column through shared memory (double buffered: one barrier per
-// step).  A pivot that is not the first largest |re| + |im| among the rows
-// still to be eliminated, or is zero, raises *vflag.
+// c - a * b (packed FMA for complex64); q = (-b.y, b.x)
+__device__ __forceinline__ float2 cfms_q(float2 c, float2 a, float2 b, float2 q) { return cfms_packed(c, a, b, q); }
+__device__ __forceinline__ double2 cfms_q(double2 c, double2 a, double2 b, double2) { return csub(c, cmul(a, b)); }
+
+// Gauss-Jordan inversion of the nb x nb (nb <= LN = InvLeaf) block at M, in
+// place.  Thread (ty, tx) of the 8 x 32 grid owns rows ty + 8 p, columns
+// tx + 32 q of an LN x LN tile padded with the identity.  Step k publishes
+// the pivot column and row (and 1 / a_kk) through shared memory, double
+// buffered so that one barrier per step suffices; every thread then applies
+// a_ij -= (a_ik / a_kk) a_kj to all its entries and the owners of row and
+// column k overwrite them with a_kj / a_kk and -a_ik / a_kk.  A pivot that is
+// zero or not the first largest |re| + |im| among the rows still to be
+// eliminated raises *vflag.
 template <typename C>
 __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __restrict__ M, long long ld,
                                                                    R_t<C> tau, int* __restrict__ vflag) {
-  constexpr int PR = kInvLeaf / 8, QC = kInvLeaf / 32;
-  __shared__ C colb[2][kInvLeaf], rowb[2][kInvLeaf];
+  constexpr int LN = InvLeaf<C>::value;
+  constexpr int PR = LN / 8, QC = LN / 32;
+  __shared__ C colb[2][LN], rowb[2][LN], pinvb[2];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   C a[PR][QC];
 #pragma unroll
@@ -2625,26 +2648,34 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
       if (ty == kr) {
 #pragma unroll
         for (int q = 0; q < QC; ++q) rowb[b][tx + 32 * q] = a[kp][q];
+        if (tx == (k & 31)) pinvb[b] = crecip_scaled(a[kp][qk]);
       }
       __syncthreads();
-      const C piv = rowb[b][k];
-      const R_t<C> pm = pmag(piv);
-      const C pinv = crecip_scaled(piv);
+      const C pinv = pinvb[b];
+      const R_t<C> pm = pmag(rowb[b][k]);
       if (k < nb && !(pm > 0)) bad = true;
+      C r[QC], rq[QC];
+#pragma unroll
+      for (int q = 0; q < QC; ++q) {
+        r[q] = rowb[b][tx + 32 * q];
+        rq[q] = cmake<C>(-r[q].y, r[q].x);
+      }
+      C f[PR];
 #pragma unroll
       for (int p = 0; p < PR; ++p) {
-        const int i = ty + 8 * p;
-        const C aik = colb[b][i];
-        if (i > k && pmag(aik) > tau * pm) bad = true;
-        const C f = cmul(aik, pinv);
-        if (p == kp && ty == kr) {  // the pivot row
+        const C aik = colb[b][ty + 8 * p];
+        if (ty + 8 * p > k && pmag(aik) > tau * pm) bad = true;
+        f[p] = cmul(aik, pinv);
 #pragma unroll
-          for (int q = 0; q < QC; ++q) a[p][q] = (tx + 32 * q == k) ? pinv : cmul(a[p][q], pinv);
-        } else {
+        for (int q = 0; q < QC; ++q) a[p][q] = cfms_q(a[p][q], f[p], r[q], rq[q]);
+      }
+      if (ty == kr) {  // row k: a_kj / a_kk
 #pragma unroll
-          for (int q = 0; q < QC; ++q)
-            a[p][q] = (tx + 32 * q == k) ? csub(czero<C>(), f) : csub(a[p][q], cmul(f, rowb[b][tx + 32 * q]));
-        }
+        for (int q = 0; q < QC; ++q) a[kp][q] = cmul(r[q], pinv);
+      }
+      if (tx == (k & 31)) {  // column k: -a_ik / a_kk, and 1 / a_kk on the diagonal
+#pragma unroll
+        for (int p = 0; p < PR; ++p) a[p][qk] = (p == kp && ty == kr) ? pinv : csub(czero<C>(), f[p]);
       }
     }
   }
@@ -2659,7 +2690,9 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
 }
 
 // scratch elements inverse_nopiv needs for an n x n matrix
+template <typename C>
 static size_t inverse_nopiv_scratch(int n) {
+  constexpr int kInvLeaf = InvLeaf<C>::value;
   size_t total = 0;
   while (n > kInvLeaf) {
     const int n1 = min(n - 1, ceil_div(n / 2, kInvLeaf) * kInvLeaf), n2 = n - n1;
@@ -2671,6 +2704,7 @@ static size_t inverse_nopiv_scratch(int n) {
 
 template <typename C>
 static int inverse_nopiv_rec(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag) {
+  constexpr int kInvLeaf = InvLeaf<C>::value;
   if (n <= kInvLeaf) {
     inv_leaf_kernel<C><<<1, kInvLeafThreads, 0, ctx.stream>>>(n, M, ld, (R_t<C>)ctx.pivot_tau, vflag);
     BEM_LAUNCH_CHECK();
@@ -2744,13 +2778,13 @@ __global__ void __launch_bounds__(1024) probe_check_kernel(int n, const C* __res
 
 template <typename C>
 size_t inverse_nopiv_scratch_elems(int n) {
-  return inverse_nopiv_scratch(n) + 3 * (size_t)n + 64;
+  return inverse_nopiv_scratch<C>(n) + 3 * (size_t)n + 64;
 }
 
 template <typename C>
 int inverse_nopiv(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag, double tol) {
   BEM_REQUIRE(n > 0 && M && ws && vflag, BEM200_ERR_ARG, "inverse_nopiv: bad arguments");
-  C* v = ws + inverse_nopiv_scratch(n) + 32;
+  C* v = ws + inverse_nopiv_scratch<C>(n) + 32;
   C* y = v + n;
   C* z = y + n;
   const C one = cmake<C>(1.0, 0.0), zero = czero<C>();
