@@ -273,8 +273,16 @@ int bem200_getrs_noalloc(int dtype, int n, int nrhs, const void* LU, int64_t ld,
  * precision 0 = complex128 throughout (the drop-in FP64 path);
  * precision 1 = mixed: complex64 factors (GEMMs on `engine`) with FP64
  * residuals and iterative refinement (bem200_bem_solve_ir).
+ * precision 2 = mixed with explicit complex64 inverses G1^-1, G2^-1,
+ * Delta^-1, Sigma^-1 (block Schur complement without pivoting, each checked
+ * by a probe M^-1 (M v) = v): every solve and refinement sweep is then a
+ * few matrix products.  bem200_bem_init returns BEM200_ERR_PIVOTING when a
+ * probe fails; write the slots again and initialise with precision 1.  The
+ * same workspace serves precisions 1 and 2; pass the precision the
+ * workspace was initialised with to every later call.
  * The workspace (bem200_bem_workspace_size bytes) holds the factors:
- * LU(G1), LU(G2), Sigma1 = H1 G1^-1, LU(Delta), Delta^-1, LU(Sigma) + pivots.
+ * LU(G1), LU(G2), Sigma1 = H1 G1^-1, LU(Delta), Delta^-1, LU(Sigma) + pivots
+ * (precision 2: the inverses in place of the LUs).
  * bem200_bem_slots returns where G1, G2, H1, H2 must be written (dtype of the
  * precision) before bem200_bem_init, which consumes them.
  * eps: eps_per_face = 0 -> eps1/eps2 are HOST (re, im) scalars of the inside /
@@ -338,6 +346,13 @@ int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, c
                         const void* H2, const void* b, int eps_per_face, const double* eps1, const double* eps2,
                         const double* nvec, double k0, double tol, int maxit, void* W1, void* W2, void* scratch,
                         void* gemm_ws, size_t gemm_ws_bytes, int32_t* iters, double* relres, void* stream);
+/* bem200_bem_solve_ir for a workspace of precision 1 or 2 (bem200_bem_solve_ir
+ * is the precision-1 form). */
+int bem200_bem_solve_ir_ex(int precision, int engine, int n, int npol, void* ws, const void* G1, const void* G2,
+                           const void* H1, const void* H2, const void* b, int eps_per_face, const double* eps1,
+                           const double* eps2, const double* nvec, double k0, double tol, int maxit, void* W1,
+                           void* W2, void* scratch, void* gemm_ws, size_t gemm_ws_bytes, int32_t* iters,
+                           double* relres, void* stream);
 
 /* y = M b: one application of the factors in ws (built by bem200_bem_init)
  * as the preconditioner of the iterative solver.  b: right-hand-side layout,

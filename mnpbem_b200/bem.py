@@ -85,7 +85,7 @@ class BEMRet:
     needs = {"sim": "ret"}
 
     def __init__(self, p, enei=None, precision="fp64", engine="bf16x3", ir_tol=1e-12, ir_maxit=30, gmres_ir=True,
-                 gmres_maxit=200, lu_tiles=None, pivoting="auto", **options):
+                 gmres_maxit=200, lu_tiles=None, pivoting="auto", explicit_inverses=True, **options):
         torch = _torch()
         if p is None:
             raise ValueError("BEMRet: 'p' must be a ComParticle (or compatible particle object), got None.")
@@ -115,6 +115,11 @@ class BEMRet:
         if pivoting not in ("auto", "partial"):
             raise ValueError("BEMRet: pivoting must be 'auto' or 'partial'")
         self.pivoting = pivoting
+        # mixed precision with pivoting='auto': the complex64 factors are first
+        # built as explicit inverses (G1^-1, G2^-1, Delta^-1, Sigma^-1 without
+        # pivoting, probe-checked), so that every refinement sweep is a few
+        # matrix products; if a check fails, LU factors as above
+        self.explicit_inverses = bool(explicit_inverses)
         self.last_pivoting = None
         # stage timer of init (profiling): set to (ctypes.c_float * 4)() to record the phases
         self._phase_buf = None
@@ -126,6 +131,9 @@ class BEMRet:
         n = self.n = p.n
         prec = 0 if precision == "fp64" else 1
         self._prec = prec
+        # precision code of the factors in the workspace for the library
+        # calls: 0 fp64, 1 mixed with LU factors, 2 mixed with explicit inverses
+        self._cprec = prec
         self._ws = None      # factor workspaces, allocated by the first init()
         self._nvec = torch.as_tensor(np.ascontiguousarray(p.nvec), dtype=torch.float64, device=self.dev)
         self.last_ir = None
@@ -185,8 +193,14 @@ class BEMRet:
         s = nat.stream_ptr()
         if self._prec == 1:
             self.g.bem_matrices(enei, dtype="c128", out=self._G128)
-        modes = ["diagonal", "partial"] if self.pivoting == "auto" else ["partial"]
+        if self.pivoting == "partial":
+            modes = ["partial"]
+        elif self._prec == 1 and self.explicit_inverses:
+            modes = ["inverse", "diagonal", "partial"]
+        else:
+            modes = ["diagonal", "partial"]
         for mode in modes:
+            cprec = 2 if mode == "inverse" else self._prec
             if self._prec == 0:
                 self._assemble_into_slots(enei, "c128")
             else:
@@ -194,14 +208,15 @@ class BEMRet:
                     nat.call("bem200_convert_c128_c64", n * n, nat.ptr(src), ctypes.c_void_p(dst), s)
             info = ctypes.c_int32(0)
             st = nat.lib().bem200_bem_init_ex(
-                self._prec, _ENGINES[self.engine], n, nat.ptr(self._ws), self._eps_mode, self._e1p, self._e2p,
+                cprec, _ENGINES[self.engine], n, nat.ptr(self._ws), self._eps_mode, self._e1p, self._e2p,
                 nat.ptr(self._nvec), self.k, nat.ptr(self._gws), self._gws_bytes,
-                _DIAGONAL_PIVOTS if mode == "diagonal" else 0, self._lookahead(), self._phase_buf,
+                0 if mode == "partial" else _DIAGONAL_PIVOTS, self._lookahead(), self._phase_buf,
                 ctypes.byref(info), s)
-            if st == nat.ERR_PIVOTING and mode == "diagonal":
-                continue  # a factor matrix needs row exchanges: factor again with partial pivoting
+            if st == nat.ERR_PIVOTING and mode != "partial":
+                continue  # a factor matrix needs row exchanges: the next, more general factorisation
             nat.check(st, "bem200_bem_init_ex")
             self.last_pivoting = mode
+            self._cprec = cprec
             break
         if self._phase_buf is not None:
             self.last_init_phases_ms = list(self._phase_buf)
@@ -272,11 +287,11 @@ class BEMRet:
             it = ctypes.c_int32(0)
             rr = ctypes.c_double(0)
             G = self._G128
-            st = L.bem200_bem_solve_ir(_ENGINES[self.engine], n, npol, nat.ptr(self._ws), nat.ptr(G[0]),
-                                       nat.ptr(G[1]), nat.ptr(G[2]), nat.ptr(G[3]), nat.ptr(bt), self._eps_mode,
-                                       self._e1p, self._e2p, nat.ptr(self._nvec), self.k, self.ir_tol, self.ir_maxit,
-                                       nat.ptr(W1), nat.ptr(W2), nat.ptr(scratch), nat.ptr(self._gws),
-                                       self._gws_bytes, ctypes.byref(it), ctypes.byref(rr), s)
+            st = L.bem200_bem_solve_ir_ex(self._cprec, _ENGINES[self.engine], n, npol, nat.ptr(self._ws),
+                                          nat.ptr(G[0]), nat.ptr(G[1]), nat.ptr(G[2]), nat.ptr(G[3]), nat.ptr(bt),
+                                          self._eps_mode, self._e1p, self._e2p, nat.ptr(self._nvec), self.k,
+                                          self.ir_tol, self.ir_maxit, nat.ptr(W1), nat.ptr(W2), nat.ptr(scratch),
+                                          nat.ptr(self._gws), self._gws_bytes, ctypes.byref(it), ctypes.byref(rr), s)
             self.last_ir = (int(it.value), float(rr.value), "ir")
             if st == nat.ERR_NOCONV and self.gmres_ir:
                 W1, W2 = self._gmres_refine(bt, npol, W1, W2, int(it.value))
@@ -307,7 +322,7 @@ class BEMRet:
                      ctypes.c_void_p(v.data_ptr() + 16 * 4 * np_), nat.ptr(b), nat.ptr(out), nat.ptr(ascr), s)
 
         def apply_M(v, out):
-            nat.call("bem200_bem_precond", 1, _ENGINES[self.engine], n, npol, nat.ptr(self._ws), nat.ptr(v),
+            nat.call("bem200_bem_precond", self._cprec, _ENGINES[self.engine], n, npol, nat.ptr(self._ws), nat.ptr(v),
                      self._eps_mode, self._e1p, self._e2p, nat.ptr(self._nvec), self.k, nat.ptr(out),
                      nat.ptr(pscr), nat.ptr(self._gws), self._gws_bytes, s)
 
@@ -333,7 +348,7 @@ class BEMRet:
     def check_status(self):
         """Raise if a factor met a zero pivot or a bounded device wait gave up."""
         status = ctypes.c_int32(0)
-        nat.call("bem200_bem_status", self._prec, self.n, nat.ptr(self._ws), ctypes.byref(status),
+        nat.call("bem200_bem_status", self._cprec, self.n, nat.ptr(self._ws), ctypes.byref(status),
                  nat.stream_ptr())
         if status.value != 0:
             raise RuntimeError("BEMRet: device status {} (3 = zero pivot in a factor, 5 = a bounded device wait "

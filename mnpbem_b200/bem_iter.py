@@ -294,7 +294,7 @@ class BEMRetIter:
         em, e1, e2 = self._eps_args
 
         def apply(v, out):
-            nat.call("bem200_bem_precond", bem._prec, _ENGINES[bem.engine], self.n, npol, nat.ptr(bem._ws),
+            nat.call("bem200_bem_precond", bem._cprec, _ENGINES[bem.engine], self.n, npol, nat.ptr(bem._ws),
                      nat.ptr(v), em, e1, e2, nat.ptr(bem._nvec), self.k, nat.ptr(out), nat.ptr(scr),
                      nat.ptr(bem._gws), bem._gws_bytes, nat.stream_ptr())
         return apply

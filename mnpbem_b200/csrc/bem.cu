@@ -119,9 +119,32 @@ __global__ void flag_to_info_kernel(const int* __restrict__ vflag, int* __restri
   if (*vflag) atomicExch(info, -BEM200_ERR_PIVOTING);
 }
 
-// probe tolerance of the complex64 Delta^-1 (relative to max|v|): the
+// probe tolerances of the complex64 inverses (relative to max|v|): the
 // factors only precondition the FP64 refinement
 constexpr double kDeltaProbeTol = 1e-2;
+constexpr double kInverseProbeTol = 1e-2;
+
+// the verdict flag of a checked factorisation: the first int of the LU
+// scratch after its row-map snapshots (as getrf places it)
+static int* lu_flag_of(int32_t* snap, int n) {
+  return reinterpret_cast<int*>(reinterpret_cast<char*>(snap) + align256(sizeof(int32_t) * 2 * (size_t)n));
+}
+
+// Out = A B (m x k times k x n, dense row-major), split along k into slices
+// whose tensor-core operand planes fit ctx's workspace
+template <typename C>
+static int gemm_fit(const LaContext& ctx, int m, int n, int k, const C* A, const C* B, C* Out) {
+  int kc = k;
+  if (ctx.engine != GemmEngine::kSimt)
+    while (kc > 64 && gemm_tc_workspace(m, n, kc, ctx.engine) > ctx.ws_bytes) kc = ((kc / 2 + 63) / 64) * 64;
+  const C one = cmake<C>(1.0, 0.0), zero = czero<C>();
+  for (int k0 = 0; k0 < k; k0 += kc) {
+    const int kk = min(kc, k - k0);
+    const int st = gemm<C>(ctx, m, n, kk, one, A + k0, k, B + (long long)k0 * n, n, k0 ? one : zero, Out, n);
+    if (st) return st;
+  }
+  return BEM200_OK;
+}
 
 // The factor chains of G1 and G2 are independent: LU(G2) and Sigma2 run on a
 // second (non-blocking) stream forked from the caller's stream with events, so
@@ -150,7 +173,7 @@ struct StageTimer {
 
 template <typename C>
 static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, const double* nvec, double k0,
-                      StageTimer* tm = nullptr) {
+                      StageTimer* tm = nullptr, bool inv = false) {
   BemState<C> s = state_view<C>(n, ws);
   auto mark = [&](int i) -> int {
     if (tm) BEM_CUDA_CHECK(cudaEventRecord(tm->ev[i], ctx.stream));
@@ -161,6 +184,9 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
   c.dinfo = s.info;
   c.dstatus = s.status;
   BEM_CUDA_CHECK(cudaMemsetAsync(s.info, 0, 2 * sizeof(int), ctx.stream));
+  int* vf[2] = {lu_flag_of(s.snap[0], n), lu_flag_of(s.snap[1], n)};  // verdicts of the checked factorisations
+  BEM_CUDA_CHECK(cudaMemsetAsync(vf[0], 0, sizeof(int), ctx.stream));
+  BEM_CUDA_CHECK(cudaMemsetAsync(vf[1], 0, sizeof(int), ctx.stream));
   int st;
   if ((st = mark(0))) return st;
   // a second chain needs half of the operand workspace for the largest GEMM of
@@ -182,6 +208,43 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
       c.ws_bytes = h;
       c2.ws = reinterpret_cast<char*>(ctx.ws) + h;
       c2.ws_bytes = h;
+    }
+  }
+  if constexpr (sizeof(C) == 8) {
+    if (inv) {
+      // explicit inverses (complex64): G1^-1 || G2^-1 by the block Schur
+      // complement, Sigma_i = H_i G_i^-1 as products, then Delta^-1 and
+      // Sigma^-1 the same way; every inverse is probe-checked
+      BEM_REQUIRE(inverse_nopiv_scratch_elems<C>(n) <= (size_t)n * n, BEM200_ERR_UNSUPPORTED,
+                  "bem_init: the inverse's scratch does not fit a slot");
+      if ((st = inverse_nopiv<C>(c, n, s.M[0], n, s.M[4], vf[0], kInverseProbeTol))) return st;
+      if ((st = gemm_fit<C>(c, n, n, n, s.M[2], s.M[0], s.M[4]))) return st;
+      BEM_CUDA_CHECK(cudaMemcpyAsync(s.M[2], s.M[4], sizeof(C) * nn, cudaMemcpyDeviceToDevice, c.stream));
+      if ((st = inverse_nopiv<C>(c2, n, s.M[1], n, s.M[5], vf[1], kInverseProbeTol))) return st;
+      if ((st = gemm_fit<C>(c2, n, n, n, s.M[3], s.M[1], s.M[5]))) return st;
+      BEM_CUDA_CHECK(cudaMemcpyAsync(s.M[3], s.M[5], sizeof(C) * nn, cudaMemcpyDeviceToDevice, c2.stream));
+      if (fork) {  // (without a second chain, c2 is c: same stream, whole workspace)
+        BEM_CUDA_CHECK(cudaEventRecord(fj.join, fj.side));
+        BEM_CUDA_CHECK(cudaStreamWaitEvent(ctx.stream, fj.join, 0));
+        c.ws_bytes = ctx.ws_bytes;
+      }
+      flag_to_info_kernel<<<1, 1, 0, ctx.stream>>>(vf[0], s.info);
+      flag_to_info_kernel<<<1, 1, 0, ctx.stream>>>(vf[1], s.info);
+      BEM_LAUNCH_CHECK();
+      if ((st = mark(1))) return st;
+      BEM_CUDA_CHECK(cudaMemsetAsync(vf[0], 0, sizeof(int), ctx.stream));
+      delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[5]);
+      BEM_LAUNCH_CHECK();
+      if ((st = mark(2))) return st;
+      if ((st = inverse_nopiv<C>(c, n, s.M[5], n, s.M[4], vf[0], kDeltaProbeTol))) return st;
+      if ((st = mark(3))) return st;
+      sigma_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(n, s.M[2], s.M[3], s.M[5], nvec, eps, k0 * k0,
+                                                                  s.M[6]);
+      BEM_LAUNCH_CHECK();
+      if ((st = inverse_nopiv<C>(c, n, s.M[6], n, s.M[4], vf[0], kInverseProbeTol))) return st;
+      flag_to_info_kernel<<<1, 1, 0, ctx.stream>>>(vf[0], s.info);
+      BEM_LAUNCH_CHECK();
+      return mark(4);
     }
   }
   // chain 1: LU(G1), Sigma1 = H1 G1^-1 (M5 is scratch)
@@ -207,8 +270,7 @@ static int bem_init_t(const LaContext& ctx, int n, void* ws, const EpsArg& eps, 
       // complex64 with checked diagonal pivots: Delta^-1 by the block Schur
       // complement (GEMMs) instead of LU(Delta) + two n-column triangular
       // solves; a failed probe raises the pivoting flag (-> partial pivoting)
-      int* vflag = reinterpret_cast<int*>(reinterpret_cast<char*>(s.snap[0]) +
-                                          align256(sizeof(int32_t) * 2 * (size_t)n));
+      int* vflag = vf[0];
       BEM_CUDA_CHECK(cudaMemsetAsync(vflag, 0, sizeof(int), ctx.stream));
       delta_kernel<C><<<ceil_div(nn, 256), 256, 0, ctx.stream>>>(nn, s.M[2], s.M[3], s.M[5]);
       BEM_LAUNCH_CHECK();
@@ -353,7 +415,8 @@ static size_t solve_scratch_bytes(int n, int p) {
 // in element type C.  scratch: solve_scratch_bytes.
 template <typename C>
 static int bem_solve_core(const LaContext& ctx0, int n, int p, void* ws, const C* phi, const C* a, const C* alpha,
-                          const C* De, const EpsArg& eps, const double* nvec, double k0, C* W1, C* W2, C* scratch) {
+                          const C* De, const EpsArg& eps, const double* nvec, double k0, C* W1, C* W2, C* scratch,
+                          bool inv = false) {
   BemState<C> s = state_view<C>(n, ws);
   LaContext ctx = ctx0;
   ctx.dstatus = s.status;
@@ -378,16 +441,25 @@ static int bem_solve_core(const LaContext& ctx0, int n, int p, void* ws, const C
   if ((st = gemm<C>(ctx, n, 3 * p, n, one, s.M[5], n, Am, 3 * p, zero, X, 3 * p))) return st;
   solve_rhs_sig_kernel<C><<<ceil_div(np, 256), 256, 0, st_>>>(n, p, Dm, X, nvec, eps, k0, rs);
   BEM_LAUNCH_CHECK();
-  // sig2 = Sigma^-1 rs   (in place in rs)
-  const bool di = sizeof(C) == 8;  // complex64 factors carry diagonal-block inverses
-  if ((st = solve_left<C>(ctx, n, p, s.M[6], n, s.map[3], rs, p, lscr, di ? s.dinv[4] : nullptr,
-                          di ? s.dinv[5] : nullptr)))
+  // sig2 = Sigma^-1 rs   (explicit inverse: a product into T; else in place in rs)
+  const bool di = sizeof(C) == 8;  // complex64 LU factors carry diagonal-block inverses
+  C* sig2 = rs;
+  if (inv) {
+    if ((st = gemm<C>(ctx, n, p, n, one, s.M[6], n, rs, p, zero, T, p))) return st;
+    sig2 = T;
+  } else if ((st = solve_left<C>(ctx, n, p, s.M[6], n, s.map[3], rs, p, lscr, di ? s.dinv[4] : nullptr,
+                                 di ? s.dinv[5] : nullptr))) {
     return st;
+  }
   // h2 = Delta^-1 (ik n L sig2 + Am)
-  solve_rhs_h_kernel<C><<<ceil_div(3 * np, 256), 256, 0, st_>>>(n, p, rs, Am, nvec, eps, k0, X);
+  solve_rhs_h_kernel<C><<<ceil_div(3 * np, 256), 256, 0, st_>>>(n, p, sig2, Am, nvec, eps, k0, X);
   BEM_LAUNCH_CHECK();
   if ((st = gemm<C>(ctx, n, 3 * p, n, one, s.M[5], n, X, 3 * p, zero, h2, 3 * p))) return st;
-  solve_pack_kernel<C><<<ceil_div(4 * np, 256), 256, 0, st_>>>(n, p, rs, h2, phi, a, W1, W2);
+  // explicit inverses: [sig2 + phi | h2 + a] and [sig2 | h2] go to S and Am..Dm
+  // (free by now) and the G products write W1, W2
+  C* P1 = inv ? S : W1;
+  C* P2 = inv ? Am : W2;
+  solve_pack_kernel<C><<<ceil_div(4 * np, 256), 256, 0, st_>>>(n, p, sig2, h2, phi, a, P1, P2);
   BEM_LAUNCH_CHECK();
   // sig1/h1 = G1^-1 W1 and sig2/h2 = G2^-1 W2 are independent: the second runs
   // on a stream forked from the caller's, with its own triangular-solve scratch
@@ -400,12 +472,17 @@ static int bem_solve_core(const LaContext& ctx0, int n, int p, void* ws, const C
   LaContext c2 = ctx;
   c2.stream = fj.side;
   void* lscr2 = reinterpret_cast<char*>(lscr) + align256(solve_left_scratch_bytes<C>(n, 4 * p));
-  if ((st = solve_left<C>(ctx, n, 4 * p, s.M[0], n, s.map[0], W1, 4 * p, lscr, di ? s.dinv[0] : nullptr,
-                          di ? s.dinv[1] : nullptr)))
-    return st;
-  if ((st = solve_left<C>(c2, n, 4 * p, s.M[1], n, s.map[1], W2, 4 * p, lscr2, di ? s.dinv[2] : nullptr,
-                          di ? s.dinv[3] : nullptr)))
-    return st;
+  if (inv) {
+    if ((st = gemm<C>(ctx, n, 4 * p, n, one, s.M[0], n, P1, 4 * p, zero, W1, 4 * p))) return st;
+    if ((st = gemm<C>(c2, n, 4 * p, n, one, s.M[1], n, P2, 4 * p, zero, W2, 4 * p))) return st;
+  } else {
+    if ((st = solve_left<C>(ctx, n, 4 * p, s.M[0], n, s.map[0], W1, 4 * p, lscr, di ? s.dinv[0] : nullptr,
+                            di ? s.dinv[1] : nullptr)))
+      return st;
+    if ((st = solve_left<C>(c2, n, 4 * p, s.M[1], n, s.map[1], W2, 4 * p, lscr2, di ? s.dinv[2] : nullptr,
+                            di ? s.dinv[3] : nullptr)))
+      return st;
+  }
   BEM_CUDA_CHECK(cudaEventRecord(fj.join, fj.side));
   BEM_CUDA_CHECK(cudaStreamWaitEvent(st_, fj.join, 0));
   return BEM200_OK;
@@ -525,7 +602,7 @@ static size_t solve_T_scratch_bytes(int n, int p) {
 // cot = [W1c | W2c] (8np, solution layout) -> b (8np, right-hand-side layout)
 template <typename C>
 static int bem_solve_T_core(const LaContext& ctx0, int n, int p, void* ws, const C* cot, const EpsArg& eps,
-                            const double* nvec, double k0, C* b, void* scratch) {
+                            const double* nvec, double k0, C* b, void* scratch, bool inv = false) {
   BemState<C> s = state_view<C>(n, ws);
   LaContext ctx = ctx0;
   ctx.dstatus = s.status;
@@ -549,9 +626,18 @@ static int bem_solve_T_core(const LaContext& ctx0, int n, int p, void* ws, const
   C* De_o = b + 7 * np;
   const C one = cmake<C>(1.0, 0.0), zero = czero<C>();
   int st;
-  BEM_CUDA_CHECK(cudaMemcpyAsync(U1, cot, sizeof(C) * 8 * np, cudaMemcpyDeviceToDevice, st_));
-  if ((st = solve_left_T<C>(ctx, n, 4 * p, s.M[0], n, s.map[0], U1, 4 * p, lscr))) return st;
-  if ((st = solve_left_T<C>(ctx, n, 4 * p, s.M[1], n, s.map[1], U2, 4 * p, lscr))) return st;
+  if (inv) {  // explicit inverses: G^-T as transposed products
+    if ((st = gemm_t<C>(ctx, n, 4 * p, n, one, plain(s.M[0], n), plain(const_cast<C*>(cot), 4 * p), zero,
+                        plain(U1, 4 * p), tscr)))
+      return st;
+    if ((st = gemm_t<C>(ctx, n, 4 * p, n, one, plain(s.M[1], n), plain(const_cast<C*>(cot) + 4 * np, 4 * p), zero,
+                        plain(U2, 4 * p), tscr)))
+      return st;
+  } else {
+    BEM_CUDA_CHECK(cudaMemcpyAsync(U1, cot, sizeof(C) * 8 * np, cudaMemcpyDeviceToDevice, st_));
+    if ((st = solve_left_T<C>(ctx, n, 4 * p, s.M[0], n, s.map[0], U1, 4 * p, lscr))) return st;
+    if ((st = solve_left_T<C>(ctx, n, 4 * p, s.M[1], n, s.map[1], U2, 4 * p, lscr))) return st;
+  }
   tsolve_start_kernel<C><<<ceil_div(4 * np, 256), 256, 0, st_>>>(n, p, U1, U2, Bs, Bh, phi_o, a_o);
   BEM_LAUNCH_CHECK();
   // w = Delta^-T Bh
@@ -559,8 +645,13 @@ static int bem_solve_T_core(const LaContext& ctx0, int n, int p, void* ws, const
     return st;
   tsolve_addnw_kernel<C><<<ceil_div(np, 256), 256, 0, st_>>>(n, p, w, nvec, eps, k0, Bs);
   BEM_LAUNCH_CHECK();
-  // v = Sigma^-T Bs (in place)
-  if ((st = solve_left_T<C>(ctx, n, p, s.M[6], n, s.map[3], Bs, p, lscr))) return st;
+  // v = Sigma^-T Bs (in place; with the explicit inverse through VA, free until tsolve_va)
+  if (inv) {
+    BEM_CUDA_CHECK(cudaMemcpyAsync(VA, Bs, sizeof(C) * np, cudaMemcpyDeviceToDevice, st_));
+    if ((st = gemm_t<C>(ctx, n, p, n, one, plain(s.M[6], n), plain(VA, p), zero, plain(Bs, p), tscr))) return st;
+  } else if ((st = solve_left_T<C>(ctx, n, p, s.M[6], n, s.map[3], Bs, p, lscr))) {
+    return st;
+  }
   tsolve_lift_kernel<C><<<ceil_div(3 * np, 256), 256, 0, st_>>>(n, p, Bs, nvec, eps, k0, T);
   BEM_LAUNCH_CHECK();
   if ((st = gemm_t<C>(ctx, n, 3 * p, n, one, plain(s.M[5], n), plain(T, 3 * p), zero, plain(t2, 3 * p), tscr)))
@@ -866,8 +957,9 @@ int bem200_bem_init_ex(int precision, int engine, int n, void* ws, int eps_per_f
   if (phase_ms)
     for (cudaEvent_t& e : tm.ev) BEM_CUDA_CHECK(cudaEventCreate(&e));
   StageTimer* tp = phase_ms ? &tm : nullptr;
+  BEM_REQUIRE(precision >= 0 && precision <= 2, BEM200_ERR_ARG, "bem_init: unknown precision %d", precision);
   int st = precision == 0 ? bem_init_t<double2>(ctx, n, ws, eps, nvec, k0, tp)
-                          : bem_init_t<float2>(ctx, n, ws, eps, nvec, k0, tp);
+                          : bem_init_t<float2>(ctx, n, ws, eps, nvec, k0, tp, precision == 2);
   if (st) return st;
   if (phase_ms) {
     BEM_CUDA_CHECK(cudaEventSynchronize(tm.ev[4]));
@@ -1047,7 +1139,7 @@ int bem200_bem_precond(int precision, int engine, int n, int npol, void* ws, con
   c128_to_c64_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(8 * np, bb, rhs32, 1.0 / bn);
   BEM_LAUNCH_CHECK();
   if ((st = bem_solve_core<float2>(ctx, n, npol, ws, rhs32, rhs32 + np, rhs32 + 4 * np, rhs32 + 7 * np, eps, nvec,
-                                   k0, sol32, sol32 + 4 * np, core)))
+                                   k0, sol32, sol32 + 4 * np, core, precision == 2)))
     return st;
   axpy_c64_to_c128_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(8 * np, sol32, bn, yy, false);
   BEM_LAUNCH_CHECK();
@@ -1089,7 +1181,7 @@ int bem200_bem_solve_T(int precision, int engine, int n, int npol, void* ws, con
   }
   c128_to_c64_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(8 * np, (const double2*)cot, cot32, 1.0 / cn);
   BEM_LAUNCH_CHECK();
-  if ((st = bem_solve_T_core<float2>(ctx, n, npol, ws, cot32, eps, nvec, k0, b32, core))) return st;
+  if ((st = bem_solve_T_core<float2>(ctx, n, npol, ws, cot32, eps, nvec, k0, b32, core, precision == 2))) return st;
   axpy_c64_to_c128_kernel<<<ceil_div(8 * np, 256), 256, 0, ctx.stream>>>(8 * np, b32, cn, (double2*)b, false);
   BEM_LAUNCH_CHECK();
   return BEM200_OK;
@@ -1113,6 +1205,18 @@ int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, c
                         const void* H2, const void* b, int eps_per_face, const double* eps1, const double* eps2,
                         const double* nvec, double k0, double tol, int maxit, void* W1, void* W2, void* scratch,
                         void* gemm_ws, size_t gemm_ws_bytes, int32_t* iters, double* relres, void* stream) {
+  return bem200_bem_solve_ir_ex(1, engine, n, npol, ws, G1, G2, H1, H2, b, eps_per_face, eps1, eps2, nvec, k0, tol,
+                                maxit, W1, W2, scratch, gemm_ws, gemm_ws_bytes, iters, relres, stream);
+}
+
+int bem200_bem_solve_ir_ex(int precision, int engine, int n, int npol, void* ws, const void* G1, const void* G2,
+                           const void* H1, const void* H2, const void* b, int eps_per_face, const double* eps1,
+                           const double* eps2, const double* nvec, double k0, double tol, int maxit, void* W1,
+                           void* W2, void* scratch, void* gemm_ws, size_t gemm_ws_bytes, int32_t* iters,
+                           double* relres, void* stream) {
+  BEM_REQUIRE(precision == 1 || precision == 2, BEM200_ERR_ARG, "bem_solve_ir: precision %d is not mixed",
+              precision);
+  const bool inv = precision == 2;
   BEM_REQUIRE(n > 0 && npol > 0 && ws && G1 && G2 && H1 && H2 && b && W1 && W2 && scratch && iters && relres,
               BEM200_ERR_ARG, "bem_solve_ir: bad arguments");
   LaContext ctx;
@@ -1150,7 +1254,7 @@ int bem200_bem_solve_ir(int engine, int n, int npol, void* ws, const void* G1, c
     BEM_LAUNCH_CHECK();
     // rhs32 = [phi (np) | a (3np) | alpha (3np) | De (np)];  sol32 = [W1 (4np) | W2 (4np)]
     if ((st = bem_solve_core<float2>(ctx, n, npol, ws, rhs32, rhs32 + np, rhs32 + 4 * np, rhs32 + 7 * np, eps, nvec,
-                                     k0, sol32, sol32 + 4 * np, core)))
+                                     k0, sol32, sol32 + 4 * np, core, inv)))
       return st;
     axpy_c64_to_c128_kernel<<<ceil_div(8 * np, 256), 256, 0, s>>>(8 * np, sol32, rnorm, x, !first);
     BEM_LAUNCH_CHECK();

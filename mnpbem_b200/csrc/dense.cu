@@ -141,22 +141,27 @@ __global__ void __launch_bounds__(256) gemm_skinny_kernel(int m, int w, int k, C
       bs[kk][q] = (k0 + kk < k && q < w) ? B.at(k0 + kk, q) : czero<C>();
     }
     __syncthreads();
-#pragma unroll 2
+    // all of the chunk's loads of A issue before any product: KC / 32 x RW
+    // requests in flight per lane keep enough bytes moving to stream A at HBM rate
+    C a[KC / 32][RW];
+#pragma unroll
+    for (int j = 0; j < KC / 32; ++j) {
+      const int kg = k0 + lane + 32 * j;
+#pragma unroll
+      for (int r = 0; r < RW; ++r) a[j][r] = (aoff[r] >= 0 && kg < k) ? __ldcs(A.base + aoff[r] + kg) : czero<C>();
+    }
+#pragma unroll
     for (int j = 0; j < KC / 32; ++j) {
       const int kk = lane + 32 * j;
-      const int kg = k0 + kk;
-      C a[RW];
-#pragma unroll
-      for (int r = 0; r < RW; ++r) a[r] = (aoff[r] >= 0 && kg < k) ? A.base[aoff[r] + kg] : czero<C>();
 #pragma unroll
       for (int q = 0; q < W; ++q) {
         const C b = bs[kk][q];
 #pragma unroll
         for (int r = 0; r < RW; ++r) {
-          acc[r][q].x = fma(a[r].x, b.x, acc[r][q].x);
-          acc[r][q].x = fma(-a[r].y, b.y, acc[r][q].x);
-          acc[r][q].y = fma(a[r].x, b.y, acc[r][q].y);
-          acc[r][q].y = fma(a[r].y, b.x, acc[r][q].y);
+          acc[r][q].x = fma(a[j][r].x, b.x, acc[r][q].x);
+          acc[r][q].x = fma(-a[j][r].y, b.y, acc[r][q].x);
+          acc[r][q].y = fma(a[j][r].x, b.y, acc[r][q].y);
+          acc[r][q].y = fma(a[j][r].y, b.x, acc[r][q].y);
         }
       }
     }
@@ -199,10 +204,12 @@ template <typename C>
 int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv) {
   if (m <= 0 || n <= 0) return BEM200_OK;
   if (n <= 16 && k >= 256) {
-    // rows per warp: keep the partial sums of a thread within ~128 registers
-    constexpr int kRw8 = sizeof(C) == 16 ? 2 : 4, kRw16 = sizeof(C) == 16 ? 1 : 2;
-    if (n <= 8) return gemm_skinny<C, 8, kRw8>(ctx, m, n, k, alpha, A, B, beta, Cv);
-    return gemm_skinny<C, 16, kRw16>(ctx, m, n, k, alpha, A, B, beta, Cv);
+    // W: columns rounded up to 4, 8 or 16; rows per warp: few enough that
+    // many CTAs (and their loads) are resident, and the sums stay in registers
+    constexpr bool z = sizeof(C) == 16;
+    if (n <= 4) return gemm_skinny<C, 4, z ? 2 : 2>(ctx, m, n, k, alpha, A, B, beta, Cv);
+    if (n <= 8) return gemm_skinny<C, 8, z ? 1 : 2>(ctx, m, n, k, alpha, A, B, beta, Cv);
+    return gemm_skinny<C, 16, 1>(ctx, m, n, k, alpha, A, B, beta, Cv);
   }
   if constexpr (sizeof(C) == 8) {
     // the tensor-core path pays ~15 us of operand preparation and pipeline

@@ -397,7 +397,7 @@ def _transposed_solve(bem, w, npol, tol=1e-12, maxit=30):
     L = nat.lib()
     n = bem.n
     s = nat.stream_ptr()
-    prec = bem._prec
+    prec = bem._cprec
     scr = torch.empty(int(L.bem200_bem_solve_T_workspace_size(prec, n, npol)), dtype=torch.uint8, device=bem.dev)
     lam = torch.empty_like(w)
 

@@ -126,9 +126,29 @@ def test_checked_diagonal_pivots_equal_partial_pivoting(cuda, precision, case):
     cp, enei = (dimer(), 520.0) if case == "dimer" else (_cube_needing_exchanges(), 600.0)
     a_bem, a_sig, a_ext, a_sca = _run(cp, enei, precision=precision)
     b_bem, b_sig, b_ext, b_sca = _run(cp, enei, precision=precision, pivoting="partial")
-    assert a_bem.last_pivoting == ("diagonal" if case == "dimer" else "partial")
+    if precision == "fp64":
+        assert a_bem.last_pivoting == ("diagonal" if case == "dimer" else "partial")
+    elif case == "dimer":
+        assert a_bem.last_pivoting == "inverse"
+    else:  # the inverses need no pivot order, only their probes' accuracy
+        assert a_bem.last_pivoting in ("inverse", "partial")
     assert b_bem.last_pivoting == "partial"
     tol = 1e-12 if precision == "fp64" else 1e-10
     assert abs(a_ext - b_ext) <= tol * abs(b_ext)
     assert abs(a_sca - b_sca) <= tol * abs(b_sca)
     assert rel(a_sig.sig2, b_sig.sig2) < 1e3 * tol
+
+
+@pytest.mark.parametrize("explicit", [True, False], ids=["inverses", "lu"])
+def test_mixed_explicit_inverses_match_lu_factors(cuda, explicit):
+    """The mixed solver's two factor forms (explicit complex64 inverses,
+    refinement by products; LU factors, refinement by triangular solves)
+    reach the FP64 solution on the config-1 family dimer."""
+    cp = dimer()
+    bem, sig, ext, sca = _run(cp, 520.0, precision="mixed", explicit_inverses=explicit)
+    assert bem.last_pivoting == ("inverse" if explicit else "diagonal")
+    ref_bem, ref_sig, ref_ext, ref_sca = _run(cp, 520.0, precision="fp64")
+    assert abs(ext - ref_ext) <= 1e-10 * abs(ref_ext)
+    assert abs(sca - ref_sca) <= 1e-10 * abs(ref_sca)
+    assert rel(sig.sig1, ref_sig.sig1) < 1e-8 and rel(sig.h2, ref_sig.h2) < 1e-8
+    assert bem.last_ir[0] <= 8
