@@ -248,6 +248,19 @@ size_t bem200_getrs_workspace_size(int dtype, int n, int nrhs);
 int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t ld, const int32_t* rowmap,
                  void* B, int64_t ldb, void* ws, size_t ws_bytes, void* scratch, int32_t* status,
                  void* stream);
+/* A <- A^-1 in place (n x n, ld = n) without pivoting, for matrices whose
+ * partial-pivoting LU exchanges no rows (the retarded BEM's G1, G2, Delta,
+ * Sigma mostly): block Schur complement recursion (GEMMs on `engine`) with
+ * Gauss-Jordan leaves.  *info (device int32) = 0, or 1 when a leaf pivot is
+ * zero or not partial pivoting's choice, or the probe max|A^-1 (A v) - v| <=
+ * tol max|v| for a fixed pseudo-random v fails; A is then unusable.
+ * scratch: bem200_inverse_nopiv_workspace_size bytes; ws: the GEMM operand
+ * workspace (bem200_gemm_workspace_size(engine, n, n, n / 2 + 64)).
+ * Replaces the explicit inverse of BEMRet.init (mnpbem/bem/bem_ret.py:437-523,
+ * Delta^-1 via lu_solve with the identity) for the mixed path. */
+size_t bem200_inverse_nopiv_workspace_size(int dtype, int n);
+int bem200_inverse_nopiv(int dtype, int engine, int n, void* A, int64_t ld, void* ws, size_t ws_bytes, void* scratch,
+                         double tol, int32_t* info, void* stream);
 /* Same solve as bem200_getrs (CUDA-core engine), for callers that cannot
  * allocate device memory: a host program linking only this library with no
  * device allocator of its own, or a caller whose device memory belongs to

@@ -85,6 +85,9 @@ _SIGS = {
     "bem200_bem_solve_ir": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
                                            ctypes.c_int, _vp, _vp, _vp, _dbl, _dbl, ctypes.c_int, _vp, _vp, _vp, _vp,
                                            _sz, _vp, _vp, _vp]),
+    "bem200_inverse_nopiv_workspace_size": (_sz, [ctypes.c_int, ctypes.c_int]),
+    "bem200_inverse_nopiv": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int64, _vp, _sz,
+                                            _vp, _dbl, _vp, _vp]),
     "bem200_bem_solve_ir_ex": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp,
                                               _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _dbl, _dbl, ctypes.c_int,
                                               _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp]),

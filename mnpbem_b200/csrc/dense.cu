@@ -2699,14 +2699,12 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
 // scratch elements inverse_nopiv needs for an n x n matrix
 template <typename C>
 static size_t inverse_nopiv_scratch(int n) {
+  // the inverse of A runs first, from the start of the scratch; then T1, T2
+  // stay live while the inverse of S uses what follows them
   constexpr int kInvLeaf = InvLeaf<C>::value;
-  size_t total = 0;
-  while (n > kInvLeaf) {
-    const int n1 = min(n - 1, ceil_div(n / 2, kInvLeaf) * kInvLeaf), n2 = n - n1;
-    total += 2 * (size_t)n1 * n2;
-    n = n2;
-  }
-  return total;
+  if (n <= kInvLeaf) return 0;
+  const int n1 = min(n - 1, ceil_div(n / 2, kInvLeaf) * kInvLeaf), n2 = n - n1;
+  return max(inverse_nopiv_scratch<C>(n1), 2 * (size_t)n1 * n2 + inverse_nopiv_scratch<C>(n2));
 }
 
 template <typename C>
@@ -2922,6 +2920,34 @@ int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t
     return solve_left<float2>(ctx, n, nrhs, (const float2*)LU, ld, rowmap, (float2*)B, ldb, scratch);
   set_error("getrs: bad dtype %d", dtype);
   return BEM200_ERR_ARG;
+}
+
+size_t bem200_inverse_nopiv_workspace_size(int dtype, int n) {
+  if (n <= 0) return 0;
+  const size_t e = dtype == BEM200_C128 ? inverse_nopiv_scratch_elems<double2>(n) : inverse_nopiv_scratch_elems<float2>(n);
+  return e * (dtype == BEM200_C128 ? sizeof(double2) : sizeof(float2)) + 256;
+}
+
+int bem200_inverse_nopiv(int dtype, int engine, int n, void* A, int64_t ld, void* ws, size_t ws_bytes, void* scratch,
+                         double tol, int32_t* info, void* stream) {
+  BEM_REQUIRE(n > 0 && A && scratch && info && ld >= n, BEM200_ERR_ARG, "inverse_nopiv: bad arguments");
+  BEM_REQUIRE(ld == n, BEM200_ERR_UNSUPPORTED, "inverse_nopiv: ld must equal n");
+  LaContext ctx;
+  ctx.stream = (cudaStream_t)stream;
+  ctx.engine = engine_of(engine);
+  ctx.ws = ws;
+  ctx.ws_bytes = ws_bytes;
+  BEM_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), ctx.stream));
+  int st;
+  if (dtype == BEM200_C128)
+    st = inverse_nopiv<double2>(ctx, n, (double2*)A, ld, (double2*)scratch, info, tol);
+  else if (dtype == BEM200_C64)
+    st = inverse_nopiv<float2>(ctx, n, (float2*)A, ld, (float2*)scratch, info, tol);
+  else {
+    set_error("inverse_nopiv: bad dtype %d", dtype);
+    return BEM200_ERR_ARG;
+  }
+  return st;
 }
 
 }  // extern "C"

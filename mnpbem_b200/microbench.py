@@ -176,6 +176,36 @@ def case_getrf(a):
             "TFLOPs": 8.0 / 3.0 * n ** 3 / ms / 1e9, "info": int(info.item()), "backward_error": berr}
 
 
+def case_inverse(a):
+    """bem200_inverse_nopiv on a column-dominant random matrix (no row
+    exchanges needed, as the BEM factor matrices)."""
+    import torch
+    from . import _native as nat
+    n = a.n
+    dt = torch.complex128 if a.dtype == "c128" else torch.complex64
+    code = nat.C128 if a.dtype == "c128" else nat.C64
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    A0 = torch.randn(n, n, dtype=dt, device="cuda", generator=gen) + 4.0 * n ** 0.5 * torch.eye(n, dtype=dt,
+                                                                                               device="cuda")
+    A = torch.empty_like(A0)
+    L = nat.lib()
+    scr = torch.empty(int(L.bem200_inverse_nopiv_workspace_size(code, n)), dtype=torch.uint8, device="cuda")
+    wsb = int(L.bem200_gemm_workspace_size(a.engine, n, n, n // 2 + 64)) if a.engine else 0
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def go():
+        A.copy_(A0)
+        nat.call("bem200_inverse_nopiv", code, a.engine, n, nat.ptr(A), n, nat.ptr(ws), wsb, nat.ptr(scr), 1e-2,
+                 nat.ptr(info), nat.stream_ptr())
+    go()
+    ms = _timed(go, a.reps)
+    res = float((A.to(torch.complex128) @ A0.to(torch.complex128)
+                 - torch.eye(n, dtype=torch.complex128, device="cuda")).abs().max())
+    return {"case": "inverse", "n": n, "dtype": a.dtype, "engine": a.engine, "ms": ms,
+            "TFLOPs": 8.0 * n ** 3 / ms / 1e9, "info": int(info.item()), "max|A^-1 A - I|": res}
+
+
 def case_hmat(a):
     """H-matrix of the dimer's G1: build of the four BEM matrices (--fill green:
     dense leaves and ACA rows / columns computed on demand; dense: dense
@@ -459,7 +489,7 @@ def case_peaks(a):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "hmat", "iter", "large", "sweep",
+    ap.add_argument("case", choices=["step", "green", "gemm", "getrf", "inverse", "hmat", "iter", "large", "sweep",
                                            "shape", "peaks", "vgrad"])
     ap.add_argument("--faces", type=int, default=1444)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -498,7 +528,8 @@ def main(argv=None):
         raise RuntimeError("microbench needs a CUDA device")
     if a.case == "step":
         a.engine = {0: "simt", 1: "bf16x3"}[a.engine]
-    out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf, "hmat": case_hmat,
+    out = {"step": case_step, "green": case_green, "gemm": case_gemm, "getrf": case_getrf, "inverse": case_inverse,
+           "hmat": case_hmat,
            "iter": case_iter, "large": case_large, "sweep": case_sweep,
            "shape": case_shape, "peaks": case_peaks, "vgrad": case_vgrad}[a.case](a)
     print(json.dumps(out), flush=True)

@@ -345,3 +345,44 @@ def test_getrf_diagonal_pivots_zero_column(cuda, dt):
     At = _t(A)
     _, _, info = _getrf_ws(At, 0, flags=4)
     assert int(info.item()) == 201
+
+
+def _inverse_nopiv(A, engine, tol=1e-2):
+    import torch
+    n = A.shape[0]
+    code = nat.C128 if A.dtype == torch.complex128 else nat.C64
+    L = nat.lib()
+    scr = torch.empty(int(L.bem200_inverse_nopiv_workspace_size(code, n)), dtype=torch.uint8, device="cuda")
+    wsb = int(L.bem200_gemm_workspace_size(engine, n, n, n // 2 + 64)) if engine else 0
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    nat.call("bem200_inverse_nopiv", code, engine, n, nat.ptr(A), n, nat.ptr(ws), wsb, nat.ptr(scr), tol,
+             nat.ptr(info), nat.stream_ptr())
+    return int(info.item())
+
+
+@pytest.mark.parametrize("dt,engine,tol", [(np.complex128, 0, 1e-12), (np.complex64, 0, 2e-5),
+                                           (np.complex64, 1, 2e-3)], ids=["c128", "c64-simt", "c64-bf16x3"])
+@pytest.mark.parametrize("n", [100, 700, 1500])
+def test_inverse_nopiv(cuda, dt, engine, tol, n):
+    """bem200_inverse_nopiv (block Schur complement, Gauss-Jordan leaves, no
+    pivoting) on a matrix whose partial-pivoting LU exchanges no rows: the
+    inverse to the dtype's (and GEMM engine's) rounding, info = 0."""
+    A = _dominant(n, 300 + n, dt)
+    At = _t(A)
+    assert _inverse_nopiv(At, engine) == 0
+    X = At.cpu().numpy().astype(np.complex128)
+    r = np.max(np.abs(X @ A.astype(np.complex128) - np.eye(n)))
+    assert r < tol, r
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64])
+def test_inverse_nopiv_reports_needed_exchange(cuda, dt):
+    """A matrix whose elimination needs row exchanges (a plain random one,
+    and a dominant one with two rows of a leaf swapped) gets info = 1."""
+    n = 300
+    A = _rand(n, n, 301).astype(dt)
+    assert _inverse_nopiv(_t(A), 0) == 1
+    B = _dominant(n, 302, dt)
+    B[[5, 40]] = B[[40, 5]]
+    assert _inverse_nopiv(_t(B), 0) == 1
