@@ -2611,14 +2611,14 @@ int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_
 // pseudo-random v) and falls back to the pivoted LU when it fails.
 template <typename C> struct InvLeaf { static constexpr int value = 128; };
 template <> struct InvLeaf<double2> { static constexpr int value = 64; };
-constexpr int kInvLeafThreads = 256;
+constexpr int kInvLeafThreads = 512;
 
 // c - a * b (packed FMA for complex64); q = (-b.y, b.x)
 __device__ __forceinline__ float2 cfms_q(float2 c, float2 a, float2 b, float2 q) { return cfms_packed(c, a, b, q); }
 __device__ __forceinline__ double2 cfms_q(double2 c, double2 a, double2 b, double2) { return csub(c, cmul(a, b)); }
 
 // Gauss-Jordan inversion of the nb x nb (nb <= LN = InvLeaf) block at M, in
-// place.  Thread (ty, tx) of the 8 x 32 grid owns rows ty + 8 p, columns
+// place.  Thread (ty, tx) of the 16 x 32 grid owns rows ty + 16 p, columns
 // tx + 32 q of an LN x LN tile padded with the identity.  Step k publishes
 // the pivot column and row (and 1 / a_kk) through shared memory, double
 // buffered so that one barrier per step suffices; every thread then applies
@@ -2630,7 +2630,7 @@ template <typename C>
 __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __restrict__ M, long long ld,
                                                                    R_t<C> tau, int* __restrict__ vflag) {
   constexpr int LN = InvLeaf<C>::value;
-  constexpr int PR = LN / 8, QC = LN / 32;
+  constexpr int TY = kInvLeafThreads / 32, PR = LN / TY, QC = LN / 32;
   __shared__ C colb[2][LN], rowb[2][LN], pinvb[2];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   C a[PR][QC];
@@ -2638,19 +2638,19 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
   for (int p = 0; p < PR; ++p)
 #pragma unroll
     for (int q = 0; q < QC; ++q) {
-      const int i = ty + 8 * p, c = tx + 32 * q;
+      const int i = ty + TY * p, c = tx + 32 * q;
       a[p][q] = (i < nb && c < nb) ? M[(long long)i * ld + c] : (i == c ? cmake<C>(1.0, 0.0) : czero<C>());
     }
   bool bad = false;
 #pragma unroll
   for (int kp = 0; kp < PR; ++kp) {
-    const int qk = kp / 4;
+    const int qk = kp * TY / 32;
 #pragma unroll 1
-    for (int kr = 0; kr < 8; ++kr) {
-      const int k = 8 * kp + kr, b = k & 1;
+    for (int kr = 0; kr < TY; ++kr) {
+      const int k = TY * kp + kr, b = k & 1;
       if (tx == (k & 31)) {
 #pragma unroll
-        for (int p = 0; p < PR; ++p) colb[b][ty + 8 * p] = a[p][qk];
+        for (int p = 0; p < PR; ++p) colb[b][ty + TY * p] = a[p][qk];
       }
       if (ty == kr) {
 #pragma unroll
@@ -2670,8 +2670,8 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
       C f[PR];
 #pragma unroll
       for (int p = 0; p < PR; ++p) {
-        const C aik = colb[b][ty + 8 * p];
-        if (ty + 8 * p > k && pmag(aik) > tau * pm) bad = true;
+        const C aik = colb[b][ty + TY * p];
+        if (ty + TY * p > k && pmag(aik) > tau * pm) bad = true;
         f[p] = cmul(aik, pinv);
 #pragma unroll
         for (int q = 0; q < QC; ++q) a[p][q] = cfms_q(a[p][q], f[p], r[q], rq[q]);
@@ -2690,7 +2690,7 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
   for (int p = 0; p < PR; ++p)
 #pragma unroll
     for (int q = 0; q < QC; ++q) {
-      const int i = ty + 8 * p, c = tx + 32 * q;
+      const int i = ty + TY * p, c = tx + 32 * q;
       if (i < nb && c < nb) M[(long long)i * ld + c] = a[p][q];
     }
   if (__any_sync(0xffffffffu, bad) && tx == 0 && vflag) atomicExch(vflag, 1);
