@@ -109,22 +109,25 @@ def case_gemm(a):
     import torch
     from . import _native as nat
     m, n, k = a.m, a.n, a.k
+    dt = torch.complex128 if a.dtype == "c128" else torch.complex64
+    code = nat.C128 if a.dtype == "c128" else nat.C64
     gen = torch.Generator(device="cuda").manual_seed(0)
-    A = torch.randn(m, k, dtype=torch.complex64, device="cuda", generator=gen)
-    B = torch.randn(k, n, dtype=torch.complex64, device="cuda", generator=gen)
-    C = torch.zeros(m, n, dtype=torch.complex64, device="cuda")
+    A = torch.randn(m, k, dtype=dt, device="cuda", generator=gen)
+    B = torch.randn(k, n, dtype=dt, device="cuda", generator=gen)
+    C = torch.zeros(m, n, dtype=dt, device="cuda")
     wsb = int(nat.lib().bem200_gemm_workspace_size(a.engine, m, n, k))
     ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
     one = (ctypes.c_double * 2)(1.0, 0.0)
     zero = (ctypes.c_double * 2)(0.0, 0.0)
 
     def go():
-        nat.call("bem200_gemm", nat.C64, a.engine, m, n, k, one, nat.ptr(A), k, nat.ptr(B), n, zero, nat.ptr(C), n,
+        nat.call("bem200_gemm", code, a.engine, m, n, k, one, nat.ptr(A), k, nat.ptr(B), n, zero, nat.ptr(C), n,
                  nat.ptr(ws), wsb, nat.stream_ptr())
     go()
     ms = _timed(go, a.reps)
-    return {"case": "gemm", "m": m, "n": n, "k": k, "engine": a.engine, "ms": ms,
-            "complex_TFLOPs": 8.0 * m * n * k / ms / 1e9}
+    return {"case": "gemm", "m": m, "n": n, "k": k, "dtype": a.dtype, "engine": a.engine, "ms": ms,
+            "complex_TFLOPs": 8.0 * m * n * k / ms / 1e9,
+            "operand_GBs": A.element_size() * (m * k + k * n + 2 * m * n) / ms / 1e6}
 
 
 def case_getrf(a):
