@@ -122,7 +122,8 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C a
 template <typename C, int W, int RW>
 __global__ void __launch_bounds__(256) gemm_skinny_kernel(int m, int w, int k, C alpha, RowView<C> A, RowView<C> B,
                                                           C beta, RowView<C> Cv) {
-  constexpr int KC = 128;
+  // 256-wide k chunks where their B rows fit the static shared memory
+  constexpr int KC = sizeof(C) * (W + 1) * 256 <= 48 * 1024 ? 256 : 128;
   __shared__ C bs[KC][W + 1];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int row0 = (blockIdx.x * 8 + wid) * RW;
