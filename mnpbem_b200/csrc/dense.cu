@@ -199,7 +199,7 @@ static int gemm_skinny(const LaContext& ctx, int m, int n, int k, C alpha, RowVi
   return BEM200_OK;
 }
 
-constexpr double kTcMinMacs = 268435456.0;  // 2^28
+constexpr double kTcMinMacs = 16777216.0;  // 2^24
 
 template <typename C>
 int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv) {
