@@ -64,18 +64,27 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C a
   for (int i = 0; i < TM; ++i)
 #pragma unroll
     for (int j = 0; j < TM; ++j) acc[i][j] = czero<C>();
-  for (int k0 = 0; k0 < k; k0 += BK) {
-    const bool kfull = (k0 + BK) <= k;
+  // the next k-slab's operands are loaded into registers while this one is
+  // multiplied, so the global-load latency overlaps the products
+  C ra[A_LOADS], rb[B_LOADS];
+  auto fetch = [&](int k0) {
     const int gc = k0 + ac;
 #pragma unroll
-    for (int i = 0; i < A_LOADS; ++i)
-      As[ac][ar0 + i * (256 / BK)] = (aoff[i] >= 0 && (kfull || gc < k)) ? A.base[aoff[i] + gc] : czero<C>();
+    for (int i = 0; i < A_LOADS; ++i) ra[i] = (aoff[i] >= 0 && gc < k) ? A.base[aoff[i] + gc] : czero<C>();
 #pragma unroll
     for (int i = 0; i < B_LOADS; ++i) {
-      int gr = k0 + br0 + i * (256 / BN);
-      Bs[br0 + i * (256 / BN)][bc] = (gr < k && bcol_ok) ? B.at(gr, n0 + bc) : czero<C>();
+      const int gr = k0 + br0 + i * (256 / BN);
+      rb[i] = (gr < k && bcol_ok) ? B.at(gr, n0 + bc) : czero<C>();
     }
+  };
+  fetch(0);
+  for (int k0 = 0; k0 < k; k0 += BK) {
+#pragma unroll
+    for (int i = 0; i < A_LOADS; ++i) As[ac][ar0 + i * (256 / BK)] = ra[i];
+#pragma unroll
+    for (int i = 0; i < B_LOADS; ++i) Bs[br0 + i * (256 / BN)][bc] = rb[i];
     __syncthreads();
+    if (k0 + BK < k) fetch(k0 + BK);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       C a[TM], b[TM];
@@ -223,7 +232,7 @@ int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, Row
   if ((long long)ceil_div(n, 64) * ceil_div(m, 64) < 296) {  // fewer than two 64 x 64 tiles per SM
     dim3 grid(ceil_div(n, 32), ceil_div(m, 32));
     BEM_REQUIRE(grid.y <= 65535, BEM200_ERR_ARG, "gemm: m too large");
-    gemm_simt_kernel<C, BK, 2><<<grid, 256, 0, ctx.stream>>>(m, n, k, alpha, A, B, beta, Cv);
+    gemm_simt_kernel<C, 2 * BK, 2><<<grid, 256, 0, ctx.stream>>>(m, n, k, alpha, A, B, beta, Cv);
     BEM_LAUNCH_CHECK();
     return BEM200_OK;
   }
