@@ -2632,8 +2632,9 @@ __device__ __forceinline__ double2 cfms_q(double2 c, double2 a, double2 b, doubl
 // tx + 32 q of an LN x LN tile padded with the identity.  Step k publishes
 // the pivot column and row (and 1 / a_kk) through shared memory, double
 // buffered so that one barrier per step suffices; every thread then applies
-// a_ij -= (a_ik / a_kk) a_kj to all its entries and the owners of row and
-// column k overwrite them with a_kj / a_kk and -a_ik / a_kk.  A pivot that is
+// a_ij -= (a_ik / a_kk) a_kj to all its entries (the published pivot carries
+// a_kk + 1, which turns column k into -a_ik / a_kk on the way), and the
+// owners of row k overwrite it with a_kj / a_kk.  A pivot that is
 // zero or not the first largest |re| + |im| among the rows still to be
 // eliminated raises *vflag.
 template <typename C>
@@ -2642,6 +2643,7 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
   constexpr int LN = InvLeaf<C>::value;
   constexpr int TY = kInvLeafThreads / 32, PR = LN / TY, QC = LN / 32;
   __shared__ C colb[2][LN], rowb[2][LN], pinvb[2];
+  __shared__ R_t<C> pmb[2];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   C a[PR][QC];
 #pragma unroll
@@ -2663,13 +2665,19 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
         for (int p = 0; p < PR; ++p) colb[b][ty + TY * p] = a[p][qk];
       }
       if (ty == kr) {
+        // the pivot row, with a_kk + 1 in place of a_kk: a_ik - (a_ik / a_kk)(a_kk + 1)
+        // = -a_ik / a_kk is then column k's new entry, from the common update
 #pragma unroll
-        for (int q = 0; q < QC; ++q) rowb[b][tx + 32 * q] = a[kp][q];
-        if (tx == (k & 31)) pinvb[b] = crecip_scaled(a[kp][qk]);
+        for (int q = 0; q < QC; ++q)
+          rowb[b][tx + 32 * q] = (tx + 32 * q == k) ? cadd(a[kp][q], cmake<C>(1.0, 0.0)) : a[kp][q];
+        if (tx == (k & 31)) {
+          pinvb[b] = crecip_scaled(a[kp][qk]);
+          pmb[b] = pmag(a[kp][qk]);
+        }
       }
       __syncthreads();
       const C pinv = pinvb[b];
-      const R_t<C> pm = pmag(rowb[b][k]);
+      const R_t<C> pm = pmb[b];
       if (k < nb && !(pm > 0)) bad = true;
       C r[QC], rq[QC];
 #pragma unroll
@@ -2686,13 +2694,9 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
 #pragma unroll
         for (int q = 0; q < QC; ++q) a[p][q] = cfms_q(a[p][q], f[p], r[q], rq[q]);
       }
-      if (ty == kr) {  // row k: a_kj / a_kk
+      if (ty == kr) {  // row k: a_kj / a_kk, and 1 / a_kk on the diagonal
 #pragma unroll
-        for (int q = 0; q < QC; ++q) a[kp][q] = cmul(r[q], pinv);
-      }
-      if (tx == (k & 31)) {  // column k: -a_ik / a_kk, and 1 / a_kk on the diagonal
-#pragma unroll
-        for (int p = 0; p < PR; ++p) a[p][qk] = (p == kp && ty == kr) ? pinv : csub(czero<C>(), f[p]);
+        for (int q = 0; q < QC; ++q) a[kp][q] = (tx + 32 * q == k) ? pinv : cmul(r[q], pinv);
       }
     }
   }
