@@ -2619,7 +2619,7 @@ int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_
 // of the leaves' pivots can cover the rows outside them, so the caller
 // verifies the result with inverse_probe (M^-1 (M v) = v for a fixed
 // pseudo-random v) and falls back to the pivoted LU when it fails.
-template <typename C> struct InvLeaf { static constexpr int value = 128; };
+template <typename C> struct InvLeaf { static constexpr int value = 64; };
 template <> struct InvLeaf<double2> { static constexpr int value = 64; };
 constexpr int kInvLeafThreads = 512;
 
