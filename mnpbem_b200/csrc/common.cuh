@@ -26,8 +26,12 @@ const char* get_error();
   } while (0)
 
 // Kernel launches are counted (bem200_launch_count) so that callers can report
-// how many device kernels a call enqueued.
+// how many device kernels a call enqueued.  Launches recorded into a CUDA
+// graph by this thread are not counted (count_suspend); a replay counts the
+// graph's kernels (count_launches).
 void count_launch();
+void count_launches(unsigned long long n);
+void count_suspend(bool on);
 #define BEM_LAUNCH_CHECK()          \
   do {                              \
     ::bem200::count_launch();       \

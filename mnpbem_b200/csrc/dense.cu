@@ -15,6 +15,10 @@
 #include <cooperative_groups.h>
 
 #include <climits>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "dense.cuh"
 
@@ -145,14 +149,9 @@ __global__ void __launch_bounds__(256) gemm_skinny_kernel(int m, int w, int k, C
 #pragma unroll
     for (int q = 0; q < W; ++q) acc[r][q] = czero<C>();
   for (int k0 = 0; k0 < k; k0 += KC) {
-    __syncthreads();
-    for (int idx = tid; idx < KC * W; idx += 256) {
-      const int kk = idx / W, q = idx % W;
-      bs[kk][q] = (k0 + kk < k && q < w) ? B.at(k0 + kk, q) : czero<C>();
-    }
-    __syncthreads();
-    // all of the chunk's loads of A issue before any product: KC / 32 x RW
-    // requests in flight per lane keep enough bytes moving to stream A at HBM rate
+    // all of the chunk's loads of A issue first, before the B rows are staged
+    // and before any product: KC / 32 x RW requests in flight per lane, whose
+    // HBM latency overlaps the staging of B from L2
     C a[KC / 32][RW];
 #pragma unroll
     for (int j = 0; j < KC / 32; ++j) {
@@ -160,6 +159,12 @@ __global__ void __launch_bounds__(256) gemm_skinny_kernel(int m, int w, int k, C
 #pragma unroll
       for (int r = 0; r < RW; ++r) a[j][r] = (aoff[r] >= 0 && kg < k) ? __ldcs(A.base + aoff[r] + kg) : czero<C>();
     }
+    __syncthreads();
+    for (int idx = tid; idx < KC * W; idx += 256) {
+      const int kk = idx / W, q = idx % W;
+      bs[kk][q] = (k0 + kk < k && q < w) ? B.at(k0 + kk, q) : czero<C>();
+    }
+    __syncthreads();
 #pragma unroll
     for (int j = 0; j < KC / 32; ++j) {
       const int kk = lane + 32 * j;
@@ -2621,82 +2626,105 @@ int inverse(const LaContext& ctx, int n, const C* LU, long long ld, const int32_
 // pseudo-random v) and falls back to the pivoted LU when it fails.
 template <typename C> struct InvLeaf { static constexpr int value = 64; };
 template <> struct InvLeaf<double2> { static constexpr int value = 64; };
-constexpr int kInvLeafThreads = 512;
-
-// c - a * b (packed FMA for complex64); q = (-b.y, b.x)
-__device__ __forceinline__ float2 cfms_q(float2 c, float2 a, float2 b, float2 q) { return cfms_packed(c, a, b, q); }
-__device__ __forceinline__ double2 cfms_q(double2 c, double2 a, double2 b, double2) { return csub(c, cmul(a, b)); }
+constexpr int kInvLeafThreads = 128;
 
 // Gauss-Jordan inversion of the nb x nb (nb <= LN = InvLeaf) block at M, in
-// place.  Thread (ty, tx) of the 16 x 32 grid owns rows ty + 16 p, columns
-// tx + 32 q of an LN x LN tile padded with the identity.  Step k publishes
-// the pivot column and row (and 1 / a_kk) through shared memory, double
-// buffered so that one barrier per step suffices; every thread then applies
-// a_ij -= (a_ik / a_kk) a_kj to all its entries (the published pivot carries
-// a_kk + 1, which turns column k into -a_ik / a_kk on the way), and the
-// owners of row k overwrite it with a_kj / a_kk.  A pivot that is
-// zero or not the first largest |re| + |im| among the rows still to be
-// eliminated raises *vflag.
+// place.  Thread (ty, tx) of the 8 x 16 grid owns the 8 x 4 block of rows
+// ty + 8 p and columns tx + 16 q of an LN x LN tile padded with the identity:
+// a step's shared-memory reads (8 entries of the pivot column, 4 of the pivot
+// row) stay small against its 32 updates, which is what bounds a step.  Step
+// k publishes the pivot column, the pivot row (each entry beside its product
+// with i, so that the update is two packed FMAs) and 1 / a_kk through shared
+// memory, double buffered so that one barrier per step suffices; every
+// thread then applies a_ij -= (a_ik / a_kk) a_kj to its entries (the
+// published pivot carries a_kk + 1, which turns column k into -a_ik / a_kk on
+// the way), and the owners of row k overwrite it with a_kj / a_kk.  A pivot
+// that is zero or not the first largest |re| + |im| among the rows still to
+// be eliminated raises *vflag.
+template <typename C> struct LeafRow { using type = C; };            // complex128: the entry
+template <> struct LeafRow<float2> { using type = float4; };         // complex64: (a_kj, i a_kj)
+__device__ __forceinline__ void leaf_pub(float4& d, float2 r) { d = make_float4(r.x, r.y, -r.y, r.x); }
+__device__ __forceinline__ void leaf_pub(double2& d, double2 r) { d = r; }
+__device__ __forceinline__ float2 leaf_fms(float2 c, float2 f, float4 rr) {
+  return cfms_packed(c, f, make_float2(rr.x, rr.y), make_float2(rr.z, rr.w));
+}
+__device__ __forceinline__ double2 leaf_fms(double2 c, double2 f, double2 r) { return csub(c, cmul(f, r)); }
+__device__ __forceinline__ float2 leaf_val(float4 rr) { return make_float2(rr.x, rr.y); }
+__device__ __forceinline__ double2 leaf_val(double2 r) { return r; }
+// 1 / p: approximate reciprocals (two MUFU operations, scaled) for complex64
+__device__ __forceinline__ float2 leaf_recip(float2 p) {
+  const float sc = fmaxf(fabsf(p.x), fabsf(p.y));
+  if (!(sc > 0.f)) return make_float2(0.f, 0.f);
+  float rs, f;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rs) : "f"(sc));
+  const float px = p.x * rs, py = p.y * rs;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(f) : "f"(px * px + py * py));
+  f *= rs;
+  return make_float2(px * f, -py * f);
+}
+__device__ __forceinline__ double2 leaf_recip(double2 p) { return crecip_scaled(p); }
+
 template <typename C>
-__global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __restrict__ M, long long ld,
-                                                                   R_t<C> tau, int* __restrict__ vflag) {
+__global__ void __launch_bounds__(kInvLeafThreads, 1) inv_leaf_kernel(int nb, C* __restrict__ M, long long ld,
+                                                                      R_t<C> tau, int* __restrict__ vflag) {
   constexpr int LN = InvLeaf<C>::value;
-  constexpr int TY = kInvLeafThreads / 32, PR = LN / TY, QC = LN / 32;
-  __shared__ C colb[2][LN], rowb[2][LN], pinvb[2];
-  __shared__ R_t<C> pmb[2];
-  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  constexpr int TY = 8, TX = 16;            // thread grid
+  constexpr int PR = LN / TY, QC = LN / TX;  // rows and columns per thread: 8 x 4
+  using RowE = typename LeafRow<C>::type;
+  using R = R_t<C>;
+  static_assert(TY * TX == kInvLeafThreads && PR * TY == LN && QC * TX == LN && TX % TY == 0, "leaf layout");
+  __shared__ RowE rowb[2][LN];
+  __shared__ C colb[2][LN];
+  __shared__ C pinvb[2];
+  __shared__ R pmb[2];
+  const int tid = threadIdx.x, ty = tid / TX, tx = tid % TX;
   C a[PR][QC];
 #pragma unroll
   for (int p = 0; p < PR; ++p)
 #pragma unroll
     for (int q = 0; q < QC; ++q) {
-      const int i = ty + TY * p, c = tx + 32 * q;
+      const int i = ty + TY * p, c = tx + TX * q;
       a[p][q] = (i < nb && c < nb) ? M[(long long)i * ld + c] : (i == c ? cmake<C>(1.0, 0.0) : czero<C>());
     }
   bool bad = false;
 #pragma unroll
-  for (int kp = 0; kp < PR; ++kp) {
-    const int qk = kp * TY / 32;
+  for (int kp = 0; kp < PR; ++kp) {   // k = TY kp + kr: row k is row kp of thread row kr
+    const int qk = (TY * kp) / TX;   // column k is column qk of thread column k % TX
 #pragma unroll 1
     for (int kr = 0; kr < TY; ++kr) {
-      const int k = TY * kp + kr, b = k & 1;
-      if (tx == (k & 31)) {
+      const int k = TY * kp + kr, b = k & 1, kx = k % TX;
+      if (tx == kx) {
 #pragma unroll
         for (int p = 0; p < PR; ++p) colb[b][ty + TY * p] = a[p][qk];
       }
       if (ty == kr) {
-        // the pivot row, with a_kk + 1 in place of a_kk: a_ik - (a_ik / a_kk)(a_kk + 1)
-        // = -a_ik / a_kk is then column k's new entry, from the common update
 #pragma unroll
         for (int q = 0; q < QC; ++q)
-          rowb[b][tx + 32 * q] = (tx + 32 * q == k) ? cadd(a[kp][q], cmake<C>(1.0, 0.0)) : a[kp][q];
-        if (tx == (k & 31)) {
-          pinvb[b] = crecip_scaled(a[kp][qk]);
+          leaf_pub(rowb[b][tx + TX * q], (q == qk && tx == kx) ? cadd(a[kp][q], cmake<C>(1.0, 0.0)) : a[kp][q]);
+        if (tx == kx) {
+          pinvb[b] = leaf_recip(a[kp][qk]);
           pmb[b] = pmag(a[kp][qk]);
         }
       }
       __syncthreads();
       const C pinv = pinvb[b];
-      const R_t<C> pm = pmb[b];
+      const R pm = pmb[b];
       if (k < nb && !(pm > 0)) bad = true;
-      C r[QC], rq[QC];
+      RowE rr[QC];
 #pragma unroll
-      for (int q = 0; q < QC; ++q) {
-        r[q] = rowb[b][tx + 32 * q];
-        rq[q] = cmake<C>(-r[q].y, r[q].x);
-      }
-      C f[PR];
+      for (int q = 0; q < QC; ++q) rr[q] = rowb[b][tx + TX * q];
 #pragma unroll
       for (int p = 0; p < PR; ++p) {
         const C aik = colb[b][ty + TY * p];
         if (ty + TY * p > k && pmag(aik) > tau * pm) bad = true;
-        f[p] = cmul(aik, pinv);
+        if (p == kp && ty == kr) {  // row k: a_kj / a_kk, and 1 / a_kk on the diagonal
 #pragma unroll
-        for (int q = 0; q < QC; ++q) a[p][q] = cfms_q(a[p][q], f[p], r[q], rq[q]);
-      }
-      if (ty == kr) {  // row k: a_kj / a_kk, and 1 / a_kk on the diagonal
+          for (int q = 0; q < QC; ++q) a[p][q] = (q == qk && tx == kx) ? pinv : cmul(leaf_val(rr[q]), pinv);
+        } else {
+          const C f = cmul(aik, pinv);
 #pragma unroll
-        for (int q = 0; q < QC; ++q) a[kp][q] = (tx + 32 * q == k) ? pinv : cmul(r[q], pinv);
+          for (int q = 0; q < QC; ++q) a[p][q] = leaf_fms(a[p][q], f, rr[q]);
+        }
       }
     }
   }
@@ -2704,10 +2732,10 @@ __global__ void __launch_bounds__(kInvLeafThreads) inv_leaf_kernel(int nb, C* __
   for (int p = 0; p < PR; ++p)
 #pragma unroll
     for (int q = 0; q < QC; ++q) {
-      const int i = ty + TY * p, c = tx + 32 * q;
+      const int i = ty + TY * p, c = tx + TX * q;
       if (i < nb && c < nb) M[(long long)i * ld + c] = a[p][q];
     }
-  if (__any_sync(0xffffffffu, bad) && tx == 0 && vflag) atomicExch(vflag, 1);
+  if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0 && vflag) atomicExch(vflag, 1);
 }
 
 // scratch elements inverse_nopiv needs for an n x n matrix
@@ -2801,8 +2829,7 @@ size_t inverse_nopiv_scratch_elems(int n) {
 }
 
 template <typename C>
-int inverse_nopiv(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag, double tol) {
-  BEM_REQUIRE(n > 0 && M && ws && vflag, BEM200_ERR_ARG, "inverse_nopiv: bad arguments");
+static int inverse_nopiv_launch(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag, double tol) {
   C* v = ws + inverse_nopiv_scratch<C>(n) + 32;
   C* y = v + n;
   C* z = y + n;
@@ -2815,6 +2842,120 @@ int inverse_nopiv(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* v
   if ((st = gemm<C>(ctx, n, 1, n, one, M, ld, y, 1, zero, z, 1))) return st;  // z = M^-1 y
   probe_check_kernel<C><<<1, 1024, 0, ctx.stream>>>(n, v, z, tol, vflag);
   BEM_LAUNCH_CHECK();
+  return BEM200_OK;
+}
+
+// ---------------------------------------------------------------- graph replay of the inverse
+// An inverse's launch sequence is a function of its arguments alone (sizes,
+// pointers, engine, workspace, tolerances): it is recorded once per argument
+// set into a CUDA graph and replayed afterwards, so that the ~600 launches of
+// an n = 5768 inverse cost one graph launch on the host and run on the device
+// without per-launch gaps.  The recording runs on a private stream of the
+// calling thread (so the caller's stream may be the legacy default stream);
+// the replay goes to the caller's stream.  Inside a caller's own stream
+// capture, or with BEM200_NO_GRAPHS set, the launches are issued directly.
+// The cache keeps the most recently used graphs; an evicted executable graph
+// that is still in flight is freed by CUDA on completion.
+namespace {
+struct InvGraph {
+  int csize, n, engine;
+  long long ld;
+  const void *M, *ws, *tcws;
+  size_t tcws_bytes;
+  const int *vflag, *dstatus;
+  double tol;
+  float tau;
+  cudaGraphExec_t exec;
+  unsigned long long kernels, used;
+  bool same(const InvGraph& o) const {
+    return csize == o.csize && n == o.n && engine == o.engine && ld == o.ld && M == o.M && ws == o.ws &&
+           tcws == o.tcws && tcws_bytes == o.tcws_bytes && vflag == o.vflag && dstatus == o.dstatus && tol == o.tol &&
+           tau == o.tau;
+  }
+};
+std::mutex g_inv_mu;
+std::vector<InvGraph> g_inv_graphs;
+unsigned long long g_inv_tick = 0;
+constexpr size_t kInvGraphCap = 256;
+struct CaptureStream {
+  cudaStream_t s = nullptr;
+  ~CaptureStream() {
+    if (s) cudaStreamDestroy(s);
+  }
+};
+thread_local CaptureStream t_capture;
+bool inv_graphs_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("BEM200_NO_GRAPHS");
+    return !(e && *e && strcmp(e, "0") != 0);
+  }();
+  return on;
+}
+}  // namespace
+
+template <typename C>
+int inverse_nopiv(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag, double tol) {
+  BEM_REQUIRE(n > 0 && M && ws && vflag, BEM200_ERR_ARG, "inverse_nopiv: bad arguments");
+  if (!inv_graphs_enabled()) return inverse_nopiv_launch<C>(ctx, n, M, ld, ws, vflag, tol);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  BEM_CUDA_CHECK(cudaStreamIsCapturing(ctx.stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return inverse_nopiv_launch<C>(ctx, n, M, ld, ws, vflag, tol);
+  InvGraph key{(int)sizeof(C), n, (int)ctx.engine, ld, M, ws, ctx.ws, ctx.ws_bytes, vflag, ctx.dstatus, tol,
+               ctx.pivot_tau, nullptr, 0, 0};
+  {
+    std::lock_guard<std::mutex> lock(g_inv_mu);
+    for (InvGraph& g : g_inv_graphs)
+      if (g.same(key)) {
+        g.used = ++g_inv_tick;
+        BEM_CUDA_CHECK(cudaGraphLaunch(g.exec, ctx.stream));
+        count_launches(g.kernels);
+        return BEM200_OK;
+      }
+  }
+  // record (launches of this thread only, on its private stream; nothing runs yet)
+  if (!t_capture.s) BEM_CUDA_CHECK(cudaStreamCreateWithFlags(&t_capture.s, cudaStreamNonBlocking));
+  LaContext rc = ctx;
+  rc.stream = t_capture.s;
+  BEM_CUDA_CHECK(cudaStreamBeginCapture(rc.stream, cudaStreamCaptureModeThreadLocal));
+  count_suspend(true);
+  const int st = inverse_nopiv_launch<C>(rc, n, M, ld, ws, vflag, tol);
+  count_suspend(false);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(rc.stream, &graph);
+  cudaGraphExec_t exec = nullptr;
+  size_t nodes = 0;
+  unsigned long long kernels = 0;
+  bool ok = st == BEM200_OK && ce == cudaSuccess && graph;
+  if (ok) ok = cudaGraphGetNodes(graph, nullptr, &nodes) == cudaSuccess;
+  if (ok && nodes) {
+    std::vector<cudaGraphNode_t> nv(nodes);
+    ok = cudaGraphGetNodes(graph, nv.data(), &nodes) == cudaSuccess;
+    for (size_t i = 0; ok && i < nodes; ++i) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nv[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+    }
+  }
+  if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (!ok) {
+    (void)cudaGetLastError();
+    if (st) return st;
+    return inverse_nopiv_launch<C>(ctx, n, M, ld, ws, vflag, tol);  // not recordable: direct launches
+  }
+  std::lock_guard<std::mutex> lock(g_inv_mu);
+  if (g_inv_graphs.size() >= kInvGraphCap) {
+    size_t lru = 0;
+    for (size_t i = 1; i < g_inv_graphs.size(); ++i)
+      if (g_inv_graphs[i].used < g_inv_graphs[lru].used) lru = i;
+    cudaGraphExecDestroy(g_inv_graphs[lru].exec);
+    g_inv_graphs.erase(g_inv_graphs.begin() + lru);
+  }
+  key.exec = exec;
+  key.kernels = kernels;
+  key.used = ++g_inv_tick;
+  g_inv_graphs.push_back(key);
+  BEM_CUDA_CHECK(cudaGraphLaunch(exec, ctx.stream));
+  count_launches(kernels);
   return BEM200_OK;
 }
 

@@ -32,7 +32,12 @@ void set_error(const char* fmt, ...) {
 const char* get_error() { return g_err; }
 
 static std::atomic<unsigned long long> g_launches{0};
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+static thread_local bool t_count_suspended = false;
+void count_launch() {
+  if (!t_count_suspended) g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void count_suspend(bool on) { t_count_suspended = on; }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 cudaError_t set_kernel_attrs(const void* kern, int smem_bytes, bool nonportable_cluster) {
