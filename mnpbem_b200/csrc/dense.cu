@@ -41,7 +41,8 @@ __device__ __forceinline__ C shfl_c(C v, int src) {
 // ===================================================================== GEMM
 // C = alpha A B + beta C on row views; block tile (16 TM) x (16 TM), each
 // thread a TM x TM register tile (rows ty + 16 i, cols tx + 16 j).  TM = 4
-// for most shapes, TM = 2 when 64 x 64 tiles would leave most SMs idle.
+// for most shapes, TM = 2 when 64 x 64 tiles would leave most SMs idle, TM = 1
+// for the small products whose 32 x 32 tiles would fill fewer than half.
 template <typename C, int BK, int TM = 4>
 __global__ void __launch_bounds__(256) gemm_simt_kernel(int m, int n, int k, C alpha, RowView<C> A, RowView<C> B,
                                                         C beta, RowView<C> Cv) {
@@ -234,6 +235,12 @@ int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, Row
       return gemm_tc_c64(ctx, m, n, k, alpha, A, B, beta, Cv);
   }
   constexpr int BK = sizeof(C) == 16 ? 8 : 16;
+  if ((long long)ceil_div(n, 32) * ceil_div(m, 32) < 74) {  // 32 x 32 tiles would fill fewer than half the SMs
+    dim3 grid(ceil_div(n, 16), ceil_div(m, 16));
+    gemm_simt_kernel<C, 32, 1><<<grid, 256, 0, ctx.stream>>>(m, n, k, alpha, A, B, beta, Cv);
+    BEM_LAUNCH_CHECK();
+    return BEM200_OK;
+  }
   if ((long long)ceil_div(n, 64) * ceil_div(m, 64) < 296) {  // fewer than two 64 x 64 tiles per SM
     dim3 grid(ceil_div(n, 32), ceil_div(m, 32));
     BEM_REQUIRE(grid.y <= 65535, BEM200_ERR_ARG, "gemm: m too large");
@@ -2713,10 +2720,11 @@ __global__ void __launch_bounds__(kInvLeafThreads, 1) inv_leaf_kernel(int nb, C*
       RowE rr[QC];
 #pragma unroll
       for (int q = 0; q < QC; ++q) rr[q] = rowb[b][tx + TX * q];
+      R lower = 0;  // largest |a_ik|_1 among this thread's rows below k
 #pragma unroll
       for (int p = 0; p < PR; ++p) {
         const C aik = colb[b][ty + TY * p];
-        if (ty + TY * p > k && pmag(aik) > tau * pm) bad = true;
+        if (p > kp || (p == kp && ty > kr)) lower = fmax(lower, pmag(aik));
         if (p == kp && ty == kr) {  // row k: a_kj / a_kk, and 1 / a_kk on the diagonal
 #pragma unroll
           for (int q = 0; q < QC; ++q) a[p][q] = (q == qk && tx == kx) ? pinv : cmul(leaf_val(rr[q]), pinv);
@@ -2726,6 +2734,7 @@ __global__ void __launch_bounds__(kInvLeafThreads, 1) inv_leaf_kernel(int nb, C*
           for (int q = 0; q < QC; ++q) a[p][q] = leaf_fms(a[p][q], f, rr[q]);
         }
       }
+      if (lower > tau * pm) bad = true;
     }
   }
 #pragma unroll
