@@ -18,6 +18,7 @@
 // Every mbarrier wait is bounded; on timeout the kernel records an error in
 // the status word, stops issuing work, waits (bounded) for its in-flight
 // copies and MMAs, frees TMEM and returns.
+#include <algorithm>
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -119,9 +120,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 }
 
 struct GemmArgs {
-  int m, n, kslabs;
+  int m, n, kslabs;     // kslabs: K slabs per split (the last split may have fewer)
+  int kslabs_total;
   float2 alpha, beta;
   RowView<float2> C;
+  float* part;          // split K: raw FP32 partial tiles [split][m][2n] (nullptr: write C)
   int* status;
 };
 
@@ -169,7 +172,8 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_bf16x3_kernel(const __grid_co
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base_sh;
-  const int nk = args.kslabs;
+  const int kb0 = blockIdx.z * args.kslabs;  // first K slab of this split
+  const int nk = max(0, min(args.kslabs, args.kslabs_total - kb0));
 
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer
@@ -183,10 +187,11 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_bf16x3_kernel(const __grid_co
       if (abort_sh) break;
       unsigned char* st = base + s * STAGE_BYTES;
       mbar_expect_tx(&full_bar[s], STAGE_BYTES);
-      tma_load_2d(&mAh, &full_bar[s], st, kb * BK, tile_m * BM);
-      tma_load_2d(&mAl, &full_bar[s], st + A_TILE, kb * BK, tile_m * BM);
-      tma_load_2d(&mBh, &full_bar[s], st + 2 * A_TILE, kb * BK, tile_n * BN);
-      tma_load_2d(&mBl, &full_bar[s], st + 2 * A_TILE + B_TILE, kb * BK, tile_n * BN);
+      const int kx = (kb0 + kb) * BK;
+      tma_load_2d(&mAh, &full_bar[s], st, kx, tile_m * BM);
+      tma_load_2d(&mAl, &full_bar[s], st + A_TILE, kx, tile_m * BM);
+      tma_load_2d(&mBh, &full_bar[s], st + 2 * A_TILE, kx, tile_n * BN);
+      tma_load_2d(&mBl, &full_bar[s], st + 2 * A_TILE + B_TILE, kx, tile_n * BN);
       issued_sh = kb + 1;
     }
   } else if (warp == 1 && lane == 0) {
@@ -235,6 +240,31 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_bf16x3_kernel(const __grid_co
     // element offset of this lane's row (row maps are read once per row)
     const long long my_off = (row_base + lane < args.m) ? args.C.off(row_base + lane, 0) : 0;
     const int nrows = min(32, args.m - row_base);
+    if (args.part) {
+      // split K: this split's raw FP32 tile, one 128-byte run of a row per
+      // thread and column block, into its slice of the partial buffer
+      const int row = row_base + lane;
+      const int n2 = 2 * args.n;
+      float* prow = args.part + ((long long)blockIdx.z * args.m + row) * n2;
+      const bool vec = (n2 & 3) == 0;
+#pragma unroll 1
+      for (int cb = 0; cb < BN / 32; ++cb) {
+        uint32_t r[32];
+        tmem_ld32(tmem + ((uint32_t)(ew * 32) << 16) + cb * 32, r);  // all lanes take part
+        const int c0 = tile_n * BN + cb * 32;
+        if (!tile_ok || row >= args.m || c0 >= n2) continue;
+        if (vec && c0 + 32 <= n2) {
+#pragma unroll
+          for (int j = 0; j < 32; j += 4)
+            *reinterpret_cast<float4*>(prow + c0 + j) = make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]),
+                                                                    __uint_as_float(r[j + 2]), __uint_as_float(r[j + 3]));
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (c0 + j < n2) prow[c0 + j] = __uint_as_float(r[j]);
+        }
+      }
+    } else {
 #pragma unroll 1
     for (int cb = 0; cb < BN / 32; ++cb) {
       uint32_t r[32];
@@ -264,6 +294,7 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_bf16x3_kernel(const __grid_co
         }
       }
       __syncwarp();
+    }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -328,6 +359,24 @@ __global__ void prep_b_kernel(int k, int n, RowView<float2> B, int Np, int Kp, _
   }
 }
 
+// split K: C = alpha (sum of the splits' partial tiles, in split order) + beta C
+__global__ void splitk_reduce_kernel(int m, int n, int splits, const float2* __restrict__ part, float2 alpha,
+                                     float2 beta, RowView<float2> C) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)m * n) return;
+  const int i = (int)(idx / n), q = (int)(idx % n);
+  float2 acc = part[idx];
+  for (int z = 1; z < splits; ++z) {
+    const float2 v = part[(long long)z * m * n + idx];
+    acc.x += v.x;
+    acc.y += v.y;
+  }
+  float2 v = cmul(alpha, acc);
+  float2& out = C.at(i, q);
+  if (beta.x != 0.f || beta.y != 0.f) v = cadd(v, cmul(beta, out));
+  out = v;
+}
+
 using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -360,8 +409,13 @@ static int make_map(CUtensorMap* m, void* ptr, int rows, int cols_bf16, int box_
 struct Plan {
   int Mp, Np, Kp;
   size_t a_bytes, b_bytes;
+  int splits, kslabs;     // K splits and slabs per split
+  size_t part_bytes;      // FP32 partial tiles of the splits (0 without split K)
 };
 
+// Products whose output tiles would occupy fewer than half of the 148 SMs
+// split K (at least 4 slabs per split, at most 8 splits), so that about one
+// CTA per SM runs; the splits' partial tiles are summed in a fixed order.
 static Plan plan(int m, int n, int k) {
   Plan p;
   p.Mp = ((m + BM - 1) / BM) * BM;
@@ -369,6 +423,12 @@ static Plan plan(int m, int n, int k) {
   p.Kp = ((2 * k + BK - 1) / BK) * BK;
   p.a_bytes = (size_t)p.Mp * p.Kp * 2;
   p.b_bytes = (size_t)p.Np * p.Kp * 2;
+  const int tiles = (p.Mp / BM) * (p.Np / BN), nk = p.Kp / BK;
+  int s = 1;
+  if (tiles < 74) s = std::min(std::min(8, std::max(1, 148 / tiles)), std::max(1, nk / 4));
+  p.kslabs = (nk + s - 1) / s;
+  p.splits = (nk + p.kslabs - 1) / p.kslabs;  // every split has at least one slab
+  p.part_bytes = p.splits > 1 ? ((size_t)p.splits * m * n * sizeof(float2) + 255) / 256 * 256 : 0;
   return p;
 }
 
@@ -377,7 +437,7 @@ static Plan plan(int m, int n, int k) {
 size_t gemm_tc_workspace(int m, int n, int k, GemmEngine e) {
   if (e == GemmEngine::kSimt) return 0;
   tc::Plan p = tc::plan(m, n, k);
-  return 2 * p.a_bytes + 2 * p.b_bytes + 4096;
+  return 2 * p.a_bytes + 2 * p.b_bytes + 4096 + p.part_bytes;
 }
 
 int gemm_tc_c64(const LaContext& ctx, int m, int n, int k, float2 alpha, RowView<float2> A, RowView<float2> B,
@@ -389,6 +449,10 @@ int gemm_tc_c64(const LaContext& ctx, int m, int n, int k, float2 alpha, RowView
   const size_t need = 2 * p.a_bytes + 2 * p.b_bytes + 4096;
   BEM_REQUIRE(ctx.ws && ctx.ws_bytes >= need, BEM200_ERR_ARG,
               "gemm_tc: workspace of %zu bytes needed for %d x %d x %d (have %zu)", need, m, n, k, ctx.ws_bytes);
+  if (p.splits > 1 && ctx.ws_bytes < need + p.part_bytes) {  // no room for the partial tiles: one split
+    p.splits = 1;
+    p.kslabs = p.Kp / BK;
+  }
   char* w = reinterpret_cast<char*>(ctx.ws);
   auto* ah = reinterpret_cast<__nv_bfloat162*>(w);
   auto* al = reinterpret_cast<__nv_bfloat162*>(w + p.a_bytes);
@@ -411,16 +475,23 @@ int gemm_tc_c64(const LaContext& ctx, int m, int n, int k, float2 alpha, RowView
   GemmArgs args;
   args.m = m;
   args.n = n;
-  args.kslabs = p.Kp / BK;
+  args.kslabs = p.kslabs;
+  args.kslabs_total = p.Kp / BK;
   args.alpha = alpha;
   args.beta = beta;
   args.C = Cv;
+  args.part = p.splits > 1 ? reinterpret_cast<float*>(w + need) : nullptr;
   args.status = status;
   BEM_CUDA_CHECK(set_kernel_attrs_once(gemm_bf16x3_kernel, SMEM_BYTES, false));
-  dim3 grid(p.Np / BN, p.Mp / BM);
+  dim3 grid(p.Np / BN, p.Mp / BM, p.splits);
   BEM_REQUIRE(grid.y <= 65535, BEM200_ERR_ARG, "gemm_tc: m too large");
   gemm_bf16x3_kernel<<<grid, THREADS, SMEM_BYTES, ctx.stream>>>(mah, mal, mbh, mbl, args);
   BEM_LAUNCH_CHECK();
+  if (p.splits > 1) {
+    splitk_reduce_kernel<<<ceil_div((long long)m * n, 256), 256, 0, ctx.stream>>>(
+        m, n, p.splits, reinterpret_cast<const float2*>(args.part), alpha, beta, Cv);
+    BEM_LAUNCH_CHECK();
+  }
   return BEM200_OK;
 }
 

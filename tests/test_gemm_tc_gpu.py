@@ -14,7 +14,9 @@ def _rand(n, m, seed):
     return (rng.standard_normal((n, m)) + 1j * rng.standard_normal((n, m))).astype(np.complex64)
 
 
-@pytest.mark.parametrize("m,n,k", [(128, 64, 64), (257, 190, 333), (1000, 700, 900), (640, 1300, 96)])
+# (1000, 700, 900) and (300, 301, 2000) split K over 3 and 8 slab ranges (odd n: scalar partial stores)
+@pytest.mark.parametrize("m,n,k", [(128, 64, 64), (257, 190, 333), (1000, 700, 900), (640, 1300, 96),
+                                   (300, 301, 2000)])
 def test_gemm_bf16x3(cuda, m, n, k):
     import torch
     A, B, C = _rand(m, k, 1), _rand(k, n, 2), _rand(m, n, 3)
