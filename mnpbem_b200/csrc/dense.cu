@@ -214,7 +214,7 @@ static int gemm_skinny(const LaContext& ctx, int m, int n, int k, C alpha, RowVi
   return BEM200_OK;
 }
 
-constexpr double kTcMinMacs = 16777216.0;  // 2^24
+constexpr double kTcMinMacs = 67108864.0;  // 2^26
 
 template <typename C>
 int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv) {
@@ -228,8 +228,9 @@ int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, Row
     return gemm_skinny<C, 16, 1>(ctx, m, n, k, alpha, A, B, beta, Cv);
   }
   if constexpr (sizeof(C) == 8) {
-    // the tensor-core path pays ~15 us of operand preparation and pipeline
-    // fill per call: below ~2^28 multiply-adds the CUDA-core tiles finish first
+    // the tensor-core path pays ~25 us of operand preparation, pipeline fill
+    // and launches per call: below ~2^26 multiply-adds (about 400^3) the
+    // CUDA-core tiles finish first
     if (ctx.engine != GemmEngine::kSimt && k >= 64 && m >= 128 && n >= 64 &&
         (double)m * n * k >= kTcMinMacs)
       return gemm_tc_c64(ctx, m, n, k, alpha, A, B, beta, Cv);

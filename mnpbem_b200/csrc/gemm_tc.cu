@@ -11,7 +11,7 @@
 // per product, FP32 accumulation).
 //
 // Kernel layout (one 128 x 256 real output tile per CTA):
-//   warp 0      : TMA producer (A_hi, A_lo, B_hi, B_lo tiles per 64-wide K slab)
+//   warp 0      : TMA producer (A_hi, A_lo, B_hi, B_lo tiles per 32-wide K slab, 4 stages)
 //   warp 1      : MMA issuer (one elected thread, tcgen05.mma kind::f16, M=128 N=256 K=16)
 //   warp 2      : TMEM allocator (256 columns)
 //   warps 4..7  : epilogue (tcgen05.ld, alpha/beta, complex64 stores via the row map)
@@ -30,13 +30,13 @@ namespace tc {
 
 constexpr int BM = 128;         // rows of the real output tile
 constexpr int BN = 256;         // real columns of the output tile (128 complex)
-constexpr int BK = 64;          // bf16 per K slab (128 bytes: one swizzle row)
-constexpr int STAGES = 2;
+constexpr int BK = 32;          // bf16 per K slab (64 bytes: one 64-byte swizzle row)
+constexpr int STAGES = 4;        // 48 KB stages: three slabs in flight behind the one multiplied
 constexpr int kGroupM = 16;       // tile rows per band of the grouped CTA order
 constexpr int UMMA_K = 16;
-constexpr int A_TILE = BM * BK * 2;   // bytes (16 KB)
-constexpr int B_TILE = BN * BK * 2;   // bytes (32 KB)
-constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;  // 96 KB
+constexpr int A_TILE = BM * BK * 2;   // bytes (8 KB)
+constexpr int B_TILE = BN * BK * 2;   // bytes (16 KB)
+constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;  // 48 KB
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr int THREADS = 256;
 constexpr long long kMaxSpin = 1LL << 26;
@@ -78,14 +78,14 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* ba
       : "memory");
 }
 
-// K-major, 128-byte swizzled operand tile: rows of 128 B, 8-row groups 1024 B apart
+// K-major, 64-byte swizzled operand tile: rows of 64 B, 8-row groups 512 B apart
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
   d |= (uint64_t)1 << 16;            // leading-dimension offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;  // stride-dimension offset: 8 rows x 128 B
+  d |= (uint64_t)(512 >> 4) << 32;   // stride-dimension offset: 8 rows x 64 B
   d |= (uint64_t)1 << 46;            // descriptor version for tcgen05
-  d |= (uint64_t)2 << 61;            // 128-byte swizzle
+  d |= (uint64_t)4 << 61;            // 64-byte swizzle
   return d;
 }
 
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_bf16x3_kernel(const __grid_co
       const uint32_t bH = smem_u32(st + 2 * A_TILE), bL = smem_u32(st + 2 * A_TILE + B_TILE);
 #pragma unroll
       for (int kk = 0; kk < BK / UMMA_K; ++kk) {
-        const uint32_t off = kk * UMMA_K * 2;  // bytes along the swizzled 128-byte row
+        const uint32_t off = kk * UMMA_K * 2;  // bytes along the swizzled 64-byte row
         const uint32_t first = (kb == 0 && kk == 0) ? 0u : 1u;
         umma(tmem, sdesc(aH + off), sdesc(bH + off), idesc, first);
         umma(tmem, sdesc(aH + off), sdesc(bL + off), idesc, 1u);
@@ -401,7 +401,7 @@ static int make_map(CUtensorMap* m, void* ptr, int rows, int cols_bf16, int box_
   cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                  CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   BEM_REQUIRE(r == CUDA_SUCCESS, BEM200_ERR_CUDA, "gemm_tc: tensor map encode failed (%d)", (int)r);
   return BEM200_OK;
 }
