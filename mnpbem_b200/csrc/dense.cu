@@ -2698,9 +2698,11 @@ __global__ void __launch_bounds__(kInvLeafThreads, 1) inv_leaf_kernel(int nb, C*
 #pragma unroll
   for (int kp = 0; kp < PR; ++kp) {   // k = TY kp + kr: row k is row kp of thread row kr
     const int qk = (TY * kp) / TX;   // column k is column qk of thread column k % TX
+    if (TY * kp >= nb) break;        // the identity padding needs no elimination steps
 #pragma unroll 1
     for (int kr = 0; kr < TY; ++kr) {
       const int k = TY * kp + kr, b = k & 1, kx = k % TX;
+      if (k >= nb) break;
       if (tx == kx) {
 #pragma unroll
         for (int p = 0; p < PR; ++p) colb[b][ty + TY * p] = a[p][qk];
