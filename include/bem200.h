@@ -256,6 +256,11 @@ int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t
  * tol max|v| for a fixed pseudo-random v fails; A is then unusable.
  * scratch: bem200_inverse_nopiv_workspace_size bytes; ws: the GEMM operand
  * workspace (bem200_gemm_workspace_size(engine, n, n, n / 2 + 64)).
+ * The launch sequence (~600 kernels at n = 5768) is recorded once per
+ * argument set (sizes, pointers, engine, workspace, tol) into a CUDA graph
+ * and replayed on `stream` afterwards; inside the caller's own stream capture,
+ * or with the environment variable BEM200_NO_GRAPHS set, the kernels are
+ * launched directly.
  * Replaces the explicit inverse of BEMRet.init (mnpbem/bem/bem_ret.py:437-523,
  * Delta^-1 via lu_solve with the identity) for the mixed path. */
 size_t bem200_inverse_nopiv_workspace_size(int dtype, int n);
