@@ -2638,27 +2638,45 @@ constexpr int kInvLeafThreads = 128;
 
 // Gauss-Jordan inversion of the nb x nb (nb <= LN = InvLeaf) block at M, in
 // place.  Thread (ty, tx) of the 8 x 16 grid owns the 8 x 4 block of rows
-// ty + 8 p and columns tx + 16 q of an LN x LN tile padded with the identity:
-// a step's shared-memory reads (8 entries of the pivot column, 4 of the pivot
-// row) stay small against its 32 updates, which is what bounds a step.  Step
-// k publishes the pivot column, the pivot row (each entry beside its product
-// with i, so that the update is two packed FMAs) and 1 / a_kk through shared
-// memory, double buffered so that one barrier per step suffices; every
-// thread then applies a_ij -= (a_ik / a_kk) a_kj to its entries (the
-// published pivot carries a_kk + 1, which turns column k into -a_ik / a_kk on
-// the way), and the owners of row k overwrite it with a_kj / a_kk.  A pivot
+// ty + 8 p and columns tx + 16 q of an LN x LN tile padded with the identity;
+// the 16 owners of a row are lanes of one warp.  Step k: the owners of row k
+// take a_kk from its lane by a shuffle, scale the row by 1 / a_kk (that is
+// the row's final value) and publish it, each entry beside its product with
+// i so that the update is two packed FMAs; the owners of column k publish it
+// (complex64: negated, each part duplicated for the packed operands).  With
+// 1 + 1 / a_kk published in place of the pivot, every other row takes
+// a_ij -= a_ik r_j, which also turns column k into -a_ik / a_kk.  The
+// buffers are double buffered, so one barrier per step suffices.  A pivot
 // that is zero or not the first largest |re| + |im| among the rows still to
 // be eliminated raises *vflag.
 template <typename C> struct LeafRow { using type = C; };            // complex128: the entry
-template <> struct LeafRow<float2> { using type = float4; };         // complex64: (a_kj, i a_kj)
+template <> struct LeafRow<float2> { using type = float4; };         // complex64: (r_j, i r_j)
+template <typename C> struct LeafCol { using type = C; };            // complex128: a_ik
+template <> struct LeafCol<float2> { using type = float4; };         // complex64: -(x, x, y, y)
 __device__ __forceinline__ void leaf_pub(float4& d, float2 r) { d = make_float4(r.x, r.y, -r.y, r.x); }
 __device__ __forceinline__ void leaf_pub(double2& d, double2 r) { d = r; }
-__device__ __forceinline__ float2 leaf_fms(float2 c, float2 f, float4 rr) {
-  return cfms_packed(c, f, make_float2(rr.x, rr.y), make_float2(rr.z, rr.w));
+__device__ __forceinline__ void leaf_pubcol(float4& d, float2 a) { d = make_float4(-a.x, -a.x, -a.y, -a.y); }
+__device__ __forceinline__ void leaf_pubcol(double2& d, double2 a) { d = a; }
+__device__ __forceinline__ float leaf_cmag(float4 c) { return fabsf(c.x) + fabsf(c.z); }
+__device__ __forceinline__ double leaf_cmag(double2 c) { return pmag(c); }
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+  return bits_f2(d);
 }
-__device__ __forceinline__ double2 leaf_fms(double2 c, double2 f, double2 r) { return csub(c, cmul(f, r)); }
-__device__ __forceinline__ float2 leaf_val(float4 rr) { return make_float2(rr.x, rr.y); }
-__device__ __forceinline__ double2 leaf_val(double2 r) { return r; }
+// a_ij - a_ik r_j over the thread's entries of one row
+template <int NQ>
+__device__ __forceinline__ void leaf_row_update(float2 (&a)[NQ], float4 c, const float4 (&rr)[NQ]) {
+  const float2 nx = make_float2(c.x, c.y), ny = make_float2(c.z, c.w);
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+    a[q] = ffma2(ny, make_float2(rr[q].z, rr[q].w), ffma2(nx, make_float2(rr[q].x, rr[q].y), a[q]));
+}
+template <int NQ>
+__device__ __forceinline__ void leaf_row_update(double2 (&a)[NQ], double2 c, const double2 (&rr)[NQ]) {
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) a[q] = csub(a[q], cmul(c, rr[q]));
+}
 // 1 / p: approximate reciprocals (two MUFU operations, scaled) for complex64
 __device__ __forceinline__ float2 leaf_recip(float2 p) {
   const float sc = fmaxf(fabsf(p.x), fabsf(p.y));
@@ -2676,16 +2694,18 @@ template <typename C>
 __global__ void __launch_bounds__(kInvLeafThreads, 1) inv_leaf_kernel(int nb, C* __restrict__ M, long long ld,
                                                                       R_t<C> tau, int* __restrict__ vflag) {
   constexpr int LN = InvLeaf<C>::value;
-  constexpr int TY = 8, TX = 16;            // thread grid
+  constexpr int TY = 8, TX = 16;             // thread grid
   constexpr int PR = LN / TY, QC = LN / TX;  // rows and columns per thread: 8 x 4
   using RowE = typename LeafRow<C>::type;
+  using ColE = typename LeafCol<C>::type;
   using R = R_t<C>;
-  static_assert(TY * TX == kInvLeafThreads && PR * TY == LN && QC * TX == LN && TX % TY == 0, "leaf layout");
+  static_assert(TY * TX == kInvLeafThreads && PR * TY == LN && QC * TX == LN && TX % TY == 0 && 32 % TX == 0,
+                "leaf layout");
   __shared__ RowE rowb[2][LN];
-  __shared__ C colb[2][LN];
-  __shared__ C pinvb[2];
+  __shared__ ColE colb[2][LN];
   __shared__ R pmb[2];
   const int tid = threadIdx.x, ty = tid / TX, tx = tid % TX;
+  const int row_lane = (tid & 31) & ~(TX - 1);  // lane of (ty, 0)
   C a[PR][QC];
 #pragma unroll
   for (int p = 0; p < PR; ++p)
@@ -2705,37 +2725,32 @@ __global__ void __launch_bounds__(kInvLeafThreads, 1) inv_leaf_kernel(int nb, C*
       if (k >= nb) break;
       if (tx == kx) {
 #pragma unroll
-        for (int p = 0; p < PR; ++p) colb[b][ty + TY * p] = a[p][qk];
+        for (int p = 0; p < PR; ++p) leaf_pubcol(colb[b][ty + TY * p], a[p][qk]);
       }
+      const C akk = shfl_c(a[kp][qk], row_lane | kx);  // a_{ty + TY kp, k}: a_kk in the lanes of row k
       if (ty == kr) {
+        const C pinv = leaf_recip(akk);
 #pragma unroll
-        for (int q = 0; q < QC; ++q)
-          leaf_pub(rowb[b][tx + TX * q], (q == qk && tx == kx) ? cadd(a[kp][q], cmake<C>(1.0, 0.0)) : a[kp][q]);
-        if (tx == kx) {
-          pinvb[b] = leaf_recip(a[kp][qk]);
-          pmb[b] = pmag(a[kp][qk]);
+        for (int q = 0; q < QC; ++q) {
+          const bool diag = q == qk && tx == kx;
+          const C r = diag ? cadd(cmake<C>(1.0, 0.0), pinv) : cmul(a[kp][q], pinv);
+          leaf_pub(rowb[b][tx + TX * q], r);
+          a[kp][q] = diag ? pinv : r;  // row k is final
         }
+        if (tx == kx) pmb[b] = pmag(akk);
       }
       __syncthreads();
-      const C pinv = pinvb[b];
       const R pm = pmb[b];
-      if (k < nb && !(pm > 0)) bad = true;
+      if (!(pm > 0)) bad = true;
       RowE rr[QC];
 #pragma unroll
       for (int q = 0; q < QC; ++q) rr[q] = rowb[b][tx + TX * q];
       R lower = 0;  // largest |a_ik|_1 among this thread's rows below k
 #pragma unroll
       for (int p = 0; p < PR; ++p) {
-        const C aik = colb[b][ty + TY * p];
-        if (p > kp || (p == kp && ty > kr)) lower = fmax(lower, pmag(aik));
-        if (p == kp && ty == kr) {  // row k: a_kj / a_kk, and 1 / a_kk on the diagonal
-#pragma unroll
-          for (int q = 0; q < QC; ++q) a[p][q] = (q == qk && tx == kx) ? pinv : cmul(leaf_val(rr[q]), pinv);
-        } else {
-          const C f = cmul(aik, pinv);
-#pragma unroll
-          for (int q = 0; q < QC; ++q) a[p][q] = leaf_fms(a[p][q], f, rr[q]);
-        }
+        const ColE cik = colb[b][ty + TY * p];
+        if (p > kp || (p == kp && ty > kr)) lower = fmax(lower, leaf_cmag(cik));
+        if (!(p == kp && ty == kr)) leaf_row_update(a[p], cik, rr);
       }
       if (lower > tau * pm) bad = true;
     }
