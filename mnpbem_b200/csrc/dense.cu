@@ -216,6 +216,18 @@ static int gemm_skinny(const LaContext& ctx, int m, int n, int k, C alpha, RowVi
 
 constexpr double kTcMinMacs = 67108864.0;  // 2^26
 
+// Whether gemm_v runs an m x n x k product on the tensor cores (the only path
+// that uses the operand workspace ctx.ws).  The tensor-core path pays ~25 us of
+// operand preparation, pipeline fill and launches per call: below ~2^26
+// multiply-adds (about 400^3) the CUDA-core tiles finish first.
+template <typename C>
+static bool gemm_takes_tc(const LaContext& ctx, int m, int n, int k) {
+  if (m <= 0 || n <= 0 || (n <= 16 && k >= 256)) return false;  // empty, or the skinny path
+  if constexpr (sizeof(C) == 8)
+    return ctx.engine != GemmEngine::kSimt && k >= 64 && m >= 128 && n >= 64 && (double)m * n * k >= kTcMinMacs;
+  return false;
+}
+
 template <typename C>
 int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, RowView<C> B, C beta, RowView<C> Cv) {
   if (m <= 0 || n <= 0) return BEM200_OK;
@@ -228,12 +240,7 @@ int gemm_v(const LaContext& ctx, int m, int n, int k, C alpha, RowView<C> A, Row
     return gemm_skinny<C, 16, 1>(ctx, m, n, k, alpha, A, B, beta, Cv);
   }
   if constexpr (sizeof(C) == 8) {
-    // the tensor-core path pays ~25 us of operand preparation, pipeline fill
-    // and launches per call: below ~2^26 multiply-adds (about 400^3) the
-    // CUDA-core tiles finish first
-    if (ctx.engine != GemmEngine::kSimt && k >= 64 && m >= 128 && n >= 64 &&
-        (double)m * n * k >= kTcMinMacs)
-      return gemm_tc_c64(ctx, m, n, k, alpha, A, B, beta, Cv);
+    if (gemm_takes_tc<C>(ctx, m, n, k)) return gemm_tc_c64(ctx, m, n, k, alpha, A, B, beta, Cv);
   }
   constexpr int BK = sizeof(C) == 16 ? 8 : 16;
   if ((long long)ceil_div(n, 32) * ceil_div(m, 32) < 74) {  // 32 x 32 tiles would fill fewer than half the SMs
@@ -2776,8 +2783,38 @@ static size_t inverse_nopiv_scratch(int n) {
   return max(inverse_nopiv_scratch<C>(n1), 2 * (size_t)n1 * n2 + inverse_nopiv_scratch<C>(n2));
 }
 
+// A side stream and two events of the recording thread: in a recorded graph
+// the recursion puts the second of two independent products on a parallel
+// branch (fork: the side stream waits for the main one; join: the reverse).
+struct RecFork {
+  cudaStream_t side;
+  cudaEvent_t fork, join;
+};
+
+// g1 on ctx.stream and g2 (given the context to launch on) either on the
+// same stream or, with fk and when neither uses the tensor-core workspace,
+// on the side stream in parallel
+template <typename C, typename F1, typename F2>
+static int gemm_pair(const LaContext& ctx, const RecFork* fk, bool tc, F1 g1, F2 g2) {
+  int st;
+  if (!fk || tc) {
+    if ((st = g1(ctx))) return st;
+    return g2(ctx);
+  }
+  LaContext side = ctx;
+  side.stream = fk->side;
+  BEM_CUDA_CHECK(cudaEventRecord(fk->fork, ctx.stream));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(fk->side, fk->fork, 0));
+  if ((st = g1(ctx))) return st;
+  if ((st = g2(side))) return st;
+  BEM_CUDA_CHECK(cudaEventRecord(fk->join, fk->side));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(ctx.stream, fk->join, 0));
+  return BEM200_OK;
+}
+
 template <typename C>
-static int inverse_nopiv_rec(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag) {
+static int inverse_nopiv_rec(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag,
+                             const RecFork* fk = nullptr) {
   constexpr int kInvLeaf = InvLeaf<C>::value;
   if (n <= kInvLeaf) {
     inv_leaf_kernel<C><<<1, kInvLeafThreads, 0, ctx.stream>>>(n, M, ld, (R_t<C>)ctx.pivot_tau, vflag);
@@ -2791,17 +2828,25 @@ static int inverse_nopiv_rec(const LaContext& ctx, int n, C* M, long long ld, C*
   C* Cm = M + (long long)n1 * ld;
   C* D = Cm + n1;
   int st;
-  if ((st = inverse_nopiv_rec<C>(ctx, n1, A, ld, ws, vflag))) return st;
+  if ((st = inverse_nopiv_rec<C>(ctx, n1, A, ld, ws, vflag, fk))) return st;
   C* T1 = ws;                            // n1 x n2
   C* T2 = ws + (size_t)n1 * n2;          // n2 x n1
   C* rest = T2 + (size_t)n2 * n1;
   const C one = cmake<C>(1.0, 0.0), mone = cmake<C>(-1.0, 0.0), zero = czero<C>();
-  if ((st = gemm<C>(ctx, n1, n2, n1, one, A, ld, B, ld, zero, T1, n2))) return st;
-  if ((st = gemm<C>(ctx, n2, n1, n1, one, Cm, ld, A, ld, zero, T2, n1))) return st;
+  // T1 = A^-1 B and T2 = C A^-1 are independent
+  const bool tc1 = gemm_takes_tc<C>(ctx, n1, n2, n1) || gemm_takes_tc<C>(ctx, n2, n1, n1);
+  if ((st = gemm_pair<C>(
+           ctx, fk, tc1, [&](const LaContext& c) { return gemm<C>(c, n1, n2, n1, one, A, ld, B, ld, zero, T1, n2); },
+           [&](const LaContext& c) { return gemm<C>(c, n2, n1, n1, one, Cm, ld, A, ld, zero, T2, n1); })))
+    return st;
   if ((st = gemm<C>(ctx, n2, n2, n1, mone, Cm, ld, T1, n2, one, D, ld))) return st;
-  if ((st = inverse_nopiv_rec<C>(ctx, n2, D, ld, rest, vflag))) return st;
-  if ((st = gemm<C>(ctx, n1, n2, n2, mone, T1, n2, D, ld, zero, B, ld))) return st;
-  if ((st = gemm<C>(ctx, n2, n1, n2, mone, D, ld, T2, n1, zero, Cm, ld))) return st;
+  if ((st = inverse_nopiv_rec<C>(ctx, n2, D, ld, rest, vflag, fk))) return st;
+  // and so are B <- -T1 S^-1 and C <- -S^-1 T2
+  const bool tc2 = gemm_takes_tc<C>(ctx, n1, n2, n2) || gemm_takes_tc<C>(ctx, n2, n1, n2);
+  if ((st = gemm_pair<C>(
+           ctx, fk, tc2, [&](const LaContext& c) { return gemm<C>(c, n1, n2, n2, mone, T1, n2, D, ld, zero, B, ld); },
+           [&](const LaContext& c) { return gemm<C>(c, n2, n1, n2, mone, D, ld, T2, n1, zero, Cm, ld); })))
+    return st;
   return gemm<C>(ctx, n1, n1, n2, mone, B, ld, T2, n1, one, A, ld);
 }
 
@@ -2856,7 +2901,8 @@ size_t inverse_nopiv_scratch_elems(int n) {
 }
 
 template <typename C>
-static int inverse_nopiv_launch(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag, double tol) {
+static int inverse_nopiv_launch(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* vflag, double tol,
+                                const RecFork* fk = nullptr) {
   C* v = ws + inverse_nopiv_scratch<C>(n) + 32;
   C* y = v + n;
   C* z = y + n;
@@ -2865,7 +2911,7 @@ static int inverse_nopiv_launch(const LaContext& ctx, int n, C* M, long long ld,
   BEM_LAUNCH_CHECK();
   int st;
   if ((st = gemm<C>(ctx, n, 1, n, one, M, ld, v, 1, zero, y, 1))) return st;  // y = M v
-  if ((st = inverse_nopiv_rec<C>(ctx, n, M, ld, ws, vflag))) return st;
+  if ((st = inverse_nopiv_rec<C>(ctx, n, M, ld, ws, vflag, fk))) return st;
   if ((st = gemm<C>(ctx, n, 1, n, one, M, ld, y, 1, zero, z, 1))) return st;  // z = M^-1 y
   probe_check_kernel<C><<<1, 1024, 0, ctx.stream>>>(n, v, z, tol, vflag);
   BEM_LAUNCH_CHECK();
@@ -2906,7 +2952,11 @@ unsigned long long g_inv_tick = 0;
 constexpr size_t kInvGraphCap = 256;
 struct CaptureStream {
   cudaStream_t s = nullptr;
+  RecFork fk{nullptr, nullptr, nullptr};
   ~CaptureStream() {
+    if (fk.fork) cudaEventDestroy(fk.fork);
+    if (fk.join) cudaEventDestroy(fk.join);
+    if (fk.side) cudaStreamDestroy(fk.side);
     if (s) cudaStreamDestroy(s);
   }
 };
@@ -2941,11 +2991,16 @@ int inverse_nopiv(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* v
   }
   // record (launches of this thread only, on its private stream; nothing runs yet)
   if (!t_capture.s) BEM_CUDA_CHECK(cudaStreamCreateWithFlags(&t_capture.s, cudaStreamNonBlocking));
+  if (!t_capture.fk.side) {
+    BEM_CUDA_CHECK(cudaStreamCreateWithFlags(&t_capture.fk.side, cudaStreamNonBlocking));
+    BEM_CUDA_CHECK(cudaEventCreateWithFlags(&t_capture.fk.fork, cudaEventDisableTiming));
+    BEM_CUDA_CHECK(cudaEventCreateWithFlags(&t_capture.fk.join, cudaEventDisableTiming));
+  }
   LaContext rc = ctx;
   rc.stream = t_capture.s;
   BEM_CUDA_CHECK(cudaStreamBeginCapture(rc.stream, cudaStreamCaptureModeThreadLocal));
   count_suspend(true);
-  const int st = inverse_nopiv_launch<C>(rc, n, M, ld, ws, vflag, tol);
+  const int st = inverse_nopiv_launch<C>(rc, n, M, ld, ws, vflag, tol, &t_capture.fk);
   count_suspend(false);
   cudaGraph_t graph = nullptr;
   const cudaError_t ce = cudaStreamEndCapture(rc.stream, &graph);
