@@ -190,8 +190,10 @@ int bem200_green_field(int n, int npart, const int32_t* pid, const int32_t* blk0
  * Building blocks of the dense BEM (reference: the LU / lu_solve / matmul
  * calls of mnpbem/bem/bem_ret.py:437-523, dispatched through
  * mnpbem/utils/gpu.py:145-279).  dtype BEM200_C128 or BEM200_C64; engine 0 =
- * CUDA cores, 1 = tcgen05 bf16x3 split (complex64 only), 2 = tcgen05 TF32
- * (complex64 only).  alpha, beta: HOST pointers to (re, im).
+ * CUDA cores, 1 = tcgen05 bf16x3 split (complex64 only); 2 is reserved for a
+ * tcgen05 TF32 engine that is not built: a product that would run on the
+ * tensor cores returns BEM200_ERR_UNSUPPORTED with it.  alpha, beta: HOST
+ * pointers to (re, im).
  * ws/ws_bytes: scratch for the tensor-core engines
  * (bem200_gemm_workspace_size), may be NULL/0 for engine 0. */
 int bem200_gemm(int dtype, int engine, int m, int n, int k, const double* alpha, const void* A, int64_t lda,

@@ -21,7 +21,7 @@ namespace bem200 {
 enum class GemmEngine : int {
   kSimt = 0,      // CUDA-core FMA (FP64 for complex128, FP32 for complex64)
   kTcBf16x3 = 1,  // complex64 on tcgen05: bf16 hi/lo split, 3 products, FP32 accumulate
-  kTcTf32 = 2,    // complex64 on tcgen05: TF32 inputs, FP32 accumulate
+  kTcTf32 = 2,    // reserved (complex64 on tcgen05 with TF32 inputs): not built, rejected by gemm_tc_c64
 };
 
 // Row-addressed matrix view: element (i, j) lives at
