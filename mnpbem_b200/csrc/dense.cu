@@ -2998,7 +2998,10 @@ int inverse_nopiv(const LaContext& ctx, int n, C* M, long long ld, C* ws, int* v
   }
   LaContext rc = ctx;
   rc.stream = t_capture.s;
-  BEM_CUDA_CHECK(cudaStreamBeginCapture(rc.stream, cudaStreamCaptureModeThreadLocal));
+  if (cudaStreamBeginCapture(rc.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return inverse_nopiv_launch<C>(ctx, n, M, ld, ws, vflag, tol);  // not recordable here: direct launches
+  }
   count_suspend(true);
   const int st = inverse_nopiv_launch<C>(rc, n, M, ld, ws, vflag, tol, &t_capture.fk);
   count_suspend(false);
