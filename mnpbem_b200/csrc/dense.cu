@@ -3163,7 +3163,7 @@ int bem200_getrs(int dtype, int engine, int n, int nrhs, const void* LU, int64_t
 }
 
 size_t bem200_inverse_nopiv_workspace_size(int dtype, int n) {
-  if (n <= 0) return 0;
+  if (n <= 0 || (dtype != BEM200_C128 && dtype != BEM200_C64)) return 0;
   const size_t e = dtype == BEM200_C128 ? inverse_nopiv_scratch_elems<double2>(n) : inverse_nopiv_scratch_elems<float2>(n);
   return e * (dtype == BEM200_C128 ? sizeof(double2) : sizeof(float2)) + 256;
 }
@@ -3172,22 +3172,15 @@ int bem200_inverse_nopiv(int dtype, int engine, int n, void* A, int64_t ld, void
                          double tol, int32_t* info, void* stream) {
   BEM_REQUIRE(n > 0 && A && scratch && info && ld >= n, BEM200_ERR_ARG, "inverse_nopiv: bad arguments");
   BEM_REQUIRE(ld == n, BEM200_ERR_UNSUPPORTED, "inverse_nopiv: ld must equal n");
+  BEM_REQUIRE(dtype == BEM200_C128 || dtype == BEM200_C64, BEM200_ERR_ARG, "inverse_nopiv: bad dtype %d", dtype);
   LaContext ctx;
   ctx.stream = (cudaStream_t)stream;
   ctx.engine = engine_of(engine);
   ctx.ws = ws;
   ctx.ws_bytes = ws_bytes;
   BEM_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), ctx.stream));
-  int st;
-  if (dtype == BEM200_C128)
-    st = inverse_nopiv<double2>(ctx, n, (double2*)A, ld, (double2*)scratch, info, tol);
-  else if (dtype == BEM200_C64)
-    st = inverse_nopiv<float2>(ctx, n, (float2*)A, ld, (float2*)scratch, info, tol);
-  else {
-    set_error("inverse_nopiv: bad dtype %d", dtype);
-    return BEM200_ERR_ARG;
-  }
-  return st;
+  if (dtype == BEM200_C128) return inverse_nopiv<double2>(ctx, n, (double2*)A, ld, (double2*)scratch, info, tol);
+  return inverse_nopiv<float2>(ctx, n, (float2*)A, ld, (float2*)scratch, info, tol);
 }
 
 }  // extern "C"
